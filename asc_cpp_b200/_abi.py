@@ -1,0 +1,172 @@
+"""ctypes declarations of the C ABI in ``include/asc_sparse_b200.h``.
+
+The structs below are field-for-field copies of the header's descriptor
+structs; ``load()`` binds every exported entry point with its exact argument
+types.  Loading fails loudly when the CUDA library has not been built -- there
+is no fallback implementation behind this module.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from enum import IntEnum
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libasc_sparse_b200.so")
+
+
+class ErrorCode(IntEnum):
+    """asc::ErrorCode (include/asc/core/status.h:35-55)."""
+    kOk = 0
+    kInvalidArgument = 1
+    kShape = 2
+    kIndex = 3
+    kOverflow = 4
+    kInvalidState = 5
+    kAllocation = 6
+    kMemoryAccess = 7
+    kMemoryTransfer = 8
+    kUnsupported = 9
+    kUnavailable = 10
+    kProvider = 11
+    kNumerical = 12
+    kInternal = 18
+
+
+class MemorySpace(IntEnum):
+    kHost = 0
+    kPinnedHost = 1
+    kDevice = 2
+    kManaged = 3
+
+
+class ElementKind(IntEnum):
+    kFloat = 0
+    kDouble = 1
+    kComplexFloat = 2
+    kComplexDouble = 3
+
+
+class FormatKind(IntEnum):
+    kCoordinate = 0
+    kCsr = 1
+    kCsc = 2
+
+
+class SparseBlasTranspose(IntEnum):
+    kNone = 0
+    kTranspose = 1
+    kConjugateTranspose = 2
+
+
+class SparseBlasLayout(IntEnum):
+    kColumnMajor = 0
+    kRowMajor = 1
+
+
+class Determinism(IntEnum):
+    kDeterministic = 0
+    kBackendDefault = 1
+
+
+class Variant(IntEnum):
+    kAuto = -1
+    kRowOrdered = 0
+    kVector = 1
+    kMergePath = 2
+    kRowSplit = 3
+
+
+PLAN_TRANSPOSE = 1
+
+
+class SparseDesc(ctypes.Structure):
+    _fields_ = [("structure_first", ctypes.c_void_p),
+                ("structure_second", ctypes.c_void_p),
+                ("values", ctypes.c_void_p),
+                ("memory_space", ctypes.c_int32),
+                ("element_kind", ctypes.c_int32),
+                ("format", ctypes.c_int32),
+                ("canonical_structure_trusted", ctypes.c_int32),
+                ("rows", ctypes.c_int64),
+                ("columns", ctypes.c_int64),
+                ("nonzeros", ctypes.c_int64)]
+
+
+class VectorDesc(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p),
+                ("reachable_data", ctypes.c_void_p),
+                ("reachable_size", ctypes.c_size_t),
+                ("memory_space", ctypes.c_int32),
+                ("element_kind", ctypes.c_int32),
+                ("extent", ctypes.c_int64),
+                ("stride", ctypes.c_int64),
+                ("writable", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+class DenseDesc(ctypes.Structure):
+    _fields_ = [("data", ctypes.c_void_p),
+                ("reachable_data", ctypes.c_void_p),
+                ("reachable_size", ctypes.c_size_t),
+                ("memory_space", ctypes.c_int32),
+                ("element_kind", ctypes.c_int32),
+                ("rows", ctypes.c_int64),
+                ("columns", ctypes.c_int64),
+                ("leading_dimension", ctypes.c_int64),
+                ("layout", ctypes.c_int32),
+                ("writable", ctypes.c_int32)]
+
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_D = ctypes.c_double
+_SZ = ctypes.c_size_t
+_SP = ctypes.POINTER(SparseDesc)
+_VP = ctypes.POINTER(VectorDesc)
+_DP = ctypes.POINTER(DenseDesc)
+
+# name -> (restype, argtypes)
+SIGNATURES: dict[str, tuple] = {
+    "asc_sb_context_create": (ctypes.c_int, [_I32, _P, ctypes.POINTER(_P)]),
+    "asc_sb_context_destroy": (ctypes.c_int, [_P]),
+    "asc_sb_context_set_determinism": (ctypes.c_int, [_P, _I32]),
+    "asc_sb_context_set_variant": (ctypes.c_int, [_P, _I32, _I32]),
+    "asc_sb_context_stream": (_P, [_P]),
+    "asc_sb_context_synchronize": (ctypes.c_int, [_P]),
+    "asc_sb_context_last_error": (ctypes.c_char_p, [_P]),
+    "asc_sb_context_launch_count": (ctypes.c_int64, [_P]),
+    "asc_sb_csr_spmv_workspace_size": (ctypes.c_int, [_P, _SP, _VP, _VP, ctypes.POINTER(_SZ)]),
+    "asc_sb_csr_spmv": (ctypes.c_int, [_P, _D, _SP, _VP, _D, _VP, _P, _SZ, _I32]),
+    "asc_sb_standard_spmv": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _VP, _VP]),
+    "asc_sb_standard_spmm": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _DP, _DP]),
+    "asc_sb_plan_workspace_size": (ctypes.c_int, [_P, _SP, _I32, ctypes.POINTER(_SZ)]),
+    "asc_sb_plan_create": (ctypes.c_int, [_P, _SP, _I32, _P, _SZ, ctypes.POINTER(_P)]),
+    "asc_sb_plan_refresh_values": (ctypes.c_int, [_P, _P]),
+    "asc_sb_plan_destroy": (ctypes.c_int, [_P]),
+    "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
+    "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
+}
+
+_lib: ctypes.CDLL | None = None
+
+
+def load(path: str | None = None) -> ctypes.CDLL:
+    """Load and bind the CUDA library; raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise ImportError(
+            f"{path} is missing: build it with `python asc_cpp_b200/build.py` "
+            "(there is no non-CUDA implementation of this library)")
+    lib = ctypes.CDLL(path)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path == LIB_PATH:
+        _lib = lib
+    return lib

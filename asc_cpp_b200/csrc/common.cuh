@@ -1,0 +1,45 @@
+// Device-side helpers shared by the sm_100a Sparse BLAS kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace ascb {
+
+// Round-to-nearest arithmetic that the compiler may not contract into an FMA.
+// The reference's x86-64 build rounds every * and + separately
+// (src/sparse/reference_blas.cc:32-37 compiled without -march), so the
+// bit-exact kernels use these exclusively.
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+
+// Streamed, read-once operands (values, column indices): evict-first so the
+// gathered x vector keeps its place in L2.
+__device__ __forceinline__ double ld_stream(const double* p) { return __ldcs(p); }
+__device__ __forceinline__ float ld_stream(const float* p) { return __ldcs(p); }
+__device__ __forceinline__ int64_t ld_stream(const int64_t* p) {
+  return static_cast<int64_t>(__ldcs(reinterpret_cast<const long long*>(p)));
+}
+
+// Gathered operand (x): read-only path, cached in L1 and L2.
+template <typename T>
+__device__ __forceinline__ T ld_gather(const T* p) { return __ldg(p); }
+
+// Strided element access; `stride` may be negative (pointer = logical 0).
+template <bool UNIT, typename T>
+__device__ __forceinline__ T& at(T* base, int64_t i, int64_t stride) {
+  return UNIT ? base[i] : base[i * stride];
+}
+template <bool UNIT, typename T>
+__device__ __forceinline__ const T& at(const T* base, int64_t i, int64_t stride) {
+  return UNIT ? base[i] : base[i * stride];
+}
+
+template <typename T>
+__device__ __forceinline__ T shfl_xor(T v, int mask, int width = 32) {
+  return __shfl_xor_sync(0xffffffffu, v, mask, width);
+}
+
+}  // namespace ascb

@@ -1,0 +1,71 @@
+// Internal launch layer: plain extern "C" entry points from the C++20 host
+// code into the sm_100a kernels.  Not part of the public ABI
+// (include/asc_sparse_b200.h is).  Every function enqueues on `stream` and
+// returns the cudaError_t of the launch (0 on success).
+#pragma once
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ascb_csr {
+  int64_t rows;
+  int64_t cols;
+  int64_t nnz;
+  const int64_t* ptr;
+  const int64_t* idx;
+  const void* val;
+} ascb_csr;
+
+typedef struct ascb_vec {
+  void* data;      // logical element 0
+  int64_t n;
+  int64_t stride;  // may be negative
+} ascb_vec;
+
+enum { ASCB_F32 = 0, ASCB_F64 = 1 };
+enum { ASCB_COL_MAJOR = 0, ASCB_ROW_MAJOR = 1 };
+// Arithmetic forms: COMPAT is y = alpha*(sum v x) + beta*y (reference_blas.cc);
+// STANDARD is y += (alpha*v)*x per entry (blas.h:1653-1665).
+enum { ASCB_COMPAT = 0, ASCB_STANDARD = 1 };
+
+// ---- partitions (integer work, bit-exact) ----
+// Row tiles of the row-ordered kernel: tile k owns rows r with
+// r + ptr[r] in [k*items, (k+1)*items).  Writes ntiles+1 row bounds.
+int64_t ascb_row_tile_count(int64_t rows, int64_t nnz, int64_t items);
+int ascb_row_tiles(void* stream, const ascb_csr* a, int64_t items,
+                   int64_t* tile_row, int64_t ntiles);
+// Merge-path split points of diagonals k*items, k = 0..ntiles (row, nnz).
+int64_t ascb_merge_tile_count(int64_t rows, int64_t nnz, int64_t items);
+int ascb_merge_path_splits(void* stream, const ascb_csr* a, int64_t items,
+                           int64_t* split_row, int64_t* split_nz,
+                           int64_t ntiles);
+
+// ---- SpMV variants ----
+// Bit-exact row-ordered SpMV (tiles from ascb_row_tiles with the same items).
+int64_t ascb_row_ordered_items(int dtype);
+int ascb_spmv_row_ordered(void* stream, int dtype, int form, const ascb_csr* a,
+                          double alpha, double beta, const ascb_vec* x,
+                          const ascb_vec* y, const int64_t* tile_row,
+                          int64_t ntiles);
+// Vector CSR: `lanes` (1..32, power of two) threads per row.
+int ascb_spmv_vector(void* stream, int dtype, int form, int lanes,
+                     const ascb_csr* a, double alpha, double beta,
+                     const ascb_vec* x, const ascb_vec* y, int sm_count);
+
+// Transposed SpMV by scatter: y[c] += alpha * v * x[r] with atomics.
+int ascb_spmv_scatter(void* stream, int dtype, const ascb_csr* a, double alpha,
+                      const ascb_vec* x, const ascb_vec* y, int sm_count);
+
+// ---- SpMM: C += alpha * op(A) * B (k right-hand sides) ----
+// transpose = 0: bit-exact stored-order kernel; 1: atomic scatter.
+int ascb_spmm(void* stream, int dtype, int transpose, const ascb_csr* a,
+              int64_t k, const void* b, int b_layout, int64_t ldb, void* c,
+              int c_layout, int64_t ldc, double alpha, int sm_count);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,327 @@
+"""Python mirror of ASCCpp's ``sparse_cuda`` facet over the C ABI.
+
+Names, argument meaning and error behaviour follow the reference's public
+templates in include/asc/sparse/providers/cuda.h:
+
+* :class:`SparseCudaContext` - ``SparseCudaContext::Create`` (cuda.h:514).
+* :func:`CudaCloneCsr` - ``CudaCloneCsr`` (cuda.h:1040-1056): copies a host
+  CSR matrix to device memory and returns a trusted device array.
+* :class:`CudaStridedVectorView` - cuda.h:616-730 (stride may also be negative
+  here, as ``SparseBlasVectorView`` allows for the standard entry points).
+* :func:`CudaCsrSpmvWorkspaceSize` / :func:`CudaCsrSpmv` - cuda.h:1758-1802.
+* :func:`CudaSpmv` / :func:`CudaSpmm` - cuda.h:1616-1658.
+
+Every failing call raises :class:`AscError` carrying the reference's
+``ErrorCode``; like the reference, a failing call has not enqueued anything.
+Device memory and streams come from torch (plumbing only); every kernel runs in
+``libasc_sparse_b200.so``.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._abi import (Determinism, ElementKind, ErrorCode, FormatKind,
+                   MemorySpace, SparseBlasLayout, SparseBlasTranspose,
+                   Variant)
+
+
+class AscError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ErrorCode(code).name}: {message}")
+        self.code = ErrorCode(code)
+        self.message = message
+
+
+def _kind(dtype: torch.dtype) -> int:
+    if dtype == torch.float64:
+        return ElementKind.kDouble
+    if dtype == torch.float32:
+        return ElementKind.kFloat
+    raise TypeError(f"unsupported element type {dtype}")
+
+
+class SparseCudaContext:
+    """Owns a library context bound to one device and one CUDA stream."""
+
+    def __init__(self, handle: int, device: int, stream):
+        self._lib = _abi.load()
+        self._h = ctypes.c_void_p(handle)
+        self.device = device
+        self._stream = stream
+
+    @classmethod
+    def Create(cls, device: int = 0, stream: torch.cuda.Stream | None = None,
+               determinism: Determinism = Determinism.kDeterministic
+               ) -> "SparseCudaContext":
+        lib = _abi.load()
+        if stream is None:
+            with torch.cuda.device(device):
+                stream = torch.cuda.Stream(device=device)
+        h = ctypes.c_void_p()
+        # handle 0 is torch's legacy default stream: pass cudaStreamLegacy (0x1),
+        # because a NULL stream asks the library to create its own.
+        raw = stream.cuda_stream or 1
+        rc = lib.asc_sb_context_create(device, ctypes.c_void_p(raw), ctypes.byref(h))
+        if rc != 0:
+            raise AscError(rc, "could not create the sparse CUDA context")
+        ctx = cls(h.value, device, stream)
+        ctx.set_determinism(determinism)
+        return ctx
+
+    # -- handle management --
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None or not self._h.value:
+            raise AscError(ErrorCode.kInvalidState,
+                           "A moved-from SparseCudaContext cannot launch work")
+        return self._h
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            self._lib.asc_sb_context_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self) -> torch.cuda.Stream:
+        return self._stream
+
+    def check(self, rc: int) -> None:
+        if rc != 0:
+            msg = self._lib.asc_sb_context_last_error(self._h)
+            raise AscError(rc, msg.decode() if msg else "")
+
+    def set_determinism(self, determinism: Determinism) -> None:
+        self.check(self._lib.asc_sb_context_set_determinism(self.handle, int(determinism)))
+
+    def set_variant(self, variant: Variant, lanes: int = 0) -> None:
+        self.check(self._lib.asc_sb_context_set_variant(self.handle, int(variant), lanes))
+
+    def synchronize(self) -> None:
+        self.check(self._lib.asc_sb_context_synchronize(self.handle))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self._lib.asc_sb_context_launch_count(self.handle))
+
+
+@dataclass
+class CudaCsrArray:
+    """Trusted device CSR (or CSC) matrix: int64 offsets/indices + values."""
+    rows: int
+    columns: int
+    offsets: torch.Tensor
+    indices: torch.Tensor
+    values: torch.Tensor
+    format: FormatKind = FormatKind.kCsr
+
+    @property
+    def nnz(self) -> int:
+        return int(self.indices.numel())
+
+    def describe(self) -> _abi.SparseDesc:
+        d = _abi.SparseDesc()
+        d.structure_first = self.offsets.data_ptr()
+        d.structure_second = self.indices.data_ptr() if self.nnz else None
+        d.values = self.values.data_ptr() if self.nnz else None
+        d.memory_space = MemorySpace.kDevice
+        d.element_kind = _kind(self.values.dtype)
+        d.format = int(self.format)
+        d.canonical_structure_trusted = 1
+        d.rows = self.rows
+        d.columns = self.columns
+        d.nonzeros = self.nnz
+        return d
+
+
+def CudaCloneCsr(context: SparseCudaContext, rows: int, columns: int,
+                 offsets: np.ndarray, indices: np.ndarray, values: np.ndarray,
+                 fmt: FormatKind = FormatKind.kCsr) -> CudaCsrArray:
+    """Host CSR -> trusted device CSR (cuda.h:1040-1056).  The structure must
+    already be canonical (the reference validates it on the host first)."""
+    dev = torch.device("cuda", context.device)
+    with torch.cuda.stream(context.stream):
+        off = torch.from_numpy(np.ascontiguousarray(offsets, np.int64)).to(dev, non_blocking=False)
+        idx = torch.from_numpy(np.ascontiguousarray(indices, np.int64)).to(dev)
+        val = torch.from_numpy(np.ascontiguousarray(values)).to(dev)
+    context.stream.synchronize()
+    return CudaCsrArray(rows, columns, off, idx, val, fmt)
+
+
+@dataclass
+class CudaStridedVectorView:
+    """``extent`` elements of ``tensor`` starting at element ``offset`` with
+    ``stride``; logical element i is storage element offset + i*stride."""
+    tensor: torch.Tensor
+    extent: int
+    stride: int = 1
+    offset: int = 0
+    writable: bool = True
+
+    @classmethod
+    def of(cls, t: torch.Tensor, writable: bool = True) -> "CudaStridedVectorView":
+        return cls(t, t.numel(), 1, 0, writable)
+
+    def describe(self) -> _abi.VectorDesc:
+        d = _abi.VectorDesc()
+        es = self.tensor.element_size()
+        d.data = self.tensor.data_ptr() + self.offset * es if self.extent else None
+        d.reachable_data = None
+        d.reachable_size = 0
+        d.memory_space = (MemorySpace.kDevice if self.tensor.is_cuda
+                          else MemorySpace.kHost)
+        d.element_kind = _kind(self.tensor.dtype)
+        d.extent = self.extent
+        d.stride = self.stride
+        d.writable = 1 if self.writable else 0
+        return d
+
+
+@dataclass
+class DenseMatrixView:
+    tensor: torch.Tensor
+    rows: int
+    columns: int
+    layout: SparseBlasLayout = SparseBlasLayout.kRowMajor
+    leading_dimension: int | None = None
+    writable: bool = True
+
+    def describe(self) -> _abi.DenseDesc:
+        d = _abi.DenseDesc()
+        d.data = self.tensor.data_ptr()
+        d.reachable_data = None
+        d.reachable_size = 0
+        d.memory_space = MemorySpace.kDevice if self.tensor.is_cuda else MemorySpace.kHost
+        d.element_kind = _kind(self.tensor.dtype)
+        d.rows = self.rows
+        d.columns = self.columns
+        if self.leading_dimension is None:
+            ld = self.columns if self.layout == SparseBlasLayout.kRowMajor else self.rows
+            ld = max(ld, 1)
+        else:
+            ld = self.leading_dimension
+        d.leading_dimension = ld
+        d.layout = int(self.layout)
+        d.writable = 1 if self.writable else 0
+        return d
+
+
+def CudaCsrSpmvWorkspaceSize(context: SparseCudaContext, matrix: CudaCsrArray,
+                             x: CudaStridedVectorView,
+                             y: CudaStridedVectorView) -> int:
+    n = ctypes.c_size_t()
+    m, xd, yd = matrix.describe(), x.describe(), y.describe()
+    xd.writable = 0
+    context.check(context._lib.asc_sb_csr_spmv_workspace_size(
+        context.handle, ctypes.byref(m), ctypes.byref(xd), ctypes.byref(yd), ctypes.byref(n)))
+    return n.value
+
+
+def CudaCsrSpmv(context: SparseCudaContext, alpha: float, matrix: CudaCsrArray,
+                x: CudaStridedVectorView, beta: float, y: CudaStridedVectorView,
+                workspace: torch.Tensor | None = None,
+                workspace_bytes: int | None = None,
+                workspace_space: MemorySpace | None = None) -> None:
+    """y = alpha*A*x + beta*y, enqueued on the context stream.  The workspace
+    placement defaults to where the workspace tensor lives."""
+    m, xd, yd = matrix.describe(), x.describe(), y.describe()
+    xd.writable = 0
+    if workspace_space is None:
+        workspace_space = (MemorySpace.kHost if workspace is not None and not workspace.is_cuda
+                           else MemorySpace.kDevice)
+    if workspace is None:
+        wptr, wbytes = None, 0 if workspace_bytes is None else workspace_bytes
+    else:
+        wptr = workspace.data_ptr()
+        wbytes = workspace.numel() * workspace.element_size() if workspace_bytes is None \
+            else workspace_bytes
+    context.check(context._lib.asc_sb_csr_spmv(
+        context.handle, float(alpha), ctypes.byref(m), ctypes.byref(xd), float(beta),
+        ctypes.byref(yd), wptr, wbytes, int(workspace_space)))
+
+
+def CudaSpmv(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
+             matrix: CudaCsrArray, x: CudaStridedVectorView,
+             y: CudaStridedVectorView, plan: "CsrPlan | None" = None) -> None:
+    """y += alpha*op(A)*x (blas.h:1607-1667 semantics)."""
+    m, xd, yd = matrix.describe(), x.describe(), y.describe()
+    xd.writable = 0
+    if plan is not None:
+        context.check(context._lib.asc_sb_plan_standard_spmv(
+            context.handle, plan.handle, int(op), float(alpha), 0.0, ctypes.byref(xd),
+            ctypes.byref(yd)))
+        return
+    context.check(context._lib.asc_sb_standard_spmv(
+        context.handle, int(op), float(alpha), 0.0, ctypes.byref(m), ctypes.byref(xd),
+        ctypes.byref(yd)))
+
+
+def CudaSpmm(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
+             matrix: CudaCsrArray, b: DenseMatrixView, c: DenseMatrixView) -> None:
+    """C += alpha*op(A)*B (blas.h:1692-1750 semantics)."""
+    m, bd, cd = matrix.describe(), b.describe(), c.describe()
+    bd.writable = 0
+    context.check(context._lib.asc_sb_standard_spmm(
+        context.handle, int(op), float(alpha), 0.0, ctypes.byref(m), ctypes.byref(bd),
+        ctypes.byref(cd)))
+
+
+class CsrPlan:
+    """Cached analysis of one device matrix (partitions, transposed structure),
+    stored in a device buffer this object owns."""
+
+    def __init__(self, context: SparseCudaContext, matrix: CudaCsrArray,
+                 flags: int = 0):
+        self.context = context
+        self.matrix = matrix
+        d = matrix.describe()
+        n = ctypes.c_size_t()
+        context.check(context._lib.asc_sb_plan_workspace_size(
+            context.handle, ctypes.byref(d), flags, ctypes.byref(n)))
+        self.buffer = torch.empty(max(n.value, 1), dtype=torch.uint8,
+                                  device=torch.device("cuda", context.device))
+        h = ctypes.c_void_p()
+        context.check(context._lib.asc_sb_plan_create(
+            context.handle, ctypes.byref(d), flags, self.buffer.data_ptr(), n.value,
+            ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def csr_spmv(self, alpha: float, x: CudaStridedVectorView, beta: float,
+                 y: CudaStridedVectorView) -> None:
+        xd, yd = x.describe(), y.describe()
+        xd.writable = 0
+        self.context.check(self.context._lib.asc_sb_plan_csr_spmv(
+            self.context.handle, self._h, float(alpha), ctypes.byref(xd), float(beta),
+            ctypes.byref(yd)))
+
+    def close(self):
+        if self._h is not None and self._h.value:
+            self.context._lib.asc_sb_plan_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

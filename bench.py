@@ -1,0 +1,357 @@
+"""Benchmark of the B200 Sparse BLAS hot path.
+
+Headline workload: FP64 CSR SpMV  y = 1.0*A*x + 0.0*y  on the 4,194,304-row
+lognormal power-law matrix (row lengths: mean 16, sigma 1.5, clipped to
+[1, 65536]; columns uniform without replacement; values N(0,1); x uniform
+[-1,1]; seed 1).  One step = one SpMV over the whole matrix.
+
+Metric: HBM GB/s by the algorithmic byte model
+    bytes = nnz*(8 + 8) + (n+1)*8 + |x| + |y|      (int64 indices, FP64)
+The inputs (1.18 GB) exceed the 126 MB L2, so no flush is needed between
+steps (x, 33.5 MB, is meant to stay L2-resident and is counted once).
+
+Arms:
+  default          : this library (C ABI), inputs resident in HBM; plus an
+                     end-to-end number through the same C ABI with x copied
+                     host->device and y device->host inside every step.
+  --impl reference : the reference's own serial CPU SpMV (compiled from its
+                     sources into oracle/_ref) over all host cores, one
+                     reference call per disjoint row block and thread.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "SpMV/SpMM HBM GB/s vs ~8 TB/s"
+WORKLOAD = "fp64_csr_spmv_powerlaw_4M"
+
+
+def _env_int(name, default):
+    try:
+        return int(os.environ.get(name, default))
+    except ValueError:
+        return default
+
+
+def _peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic_record():
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return {}
+
+
+def _host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def _matrix(seed=1):
+    from asc_cpp_b200 import synthetic
+    a = synthetic.power_law(4_194_304, 16.0, 1.5, 65_536, seed=seed, dtype=np.float64)
+    rng = np.random.default_rng(seed + 1000)
+    x = rng.uniform(-1.0, 1.0, a.cols)
+    return a, x
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.device_index = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-i", str(self.device_index), "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in getattr(self, "lines", []):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": mx or None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference(args, rank, world):
+    """--impl reference: the reference's own CPU SpMV on the host cores."""
+    if rank != 0:
+        return 0
+    from oracle import Reference, Restatement, build_oracle
+    a, x = _matrix()
+    threads = _host_threads()
+    kind = "reference"
+    if Reference.available():
+        ref = Reference()
+        handle = ref.blocks_prepare(a.rows, a.cols, a.ptr, a.idx, a.val, threads)
+        run = lambda y: ref.blocks_run(handle, np.float64, 1.0, x, 0.0, y)  # noqa: E731
+    else:  # compiled reference absent: the C restatement, serial
+        kind, threads = "port", 1
+        build_oracle.build_restatement()
+        rs = Restatement()
+        run = lambda y: rs.compat_spmv(a.ptr, a.idx, a.val, 1.0, x, 0.0, y)  # noqa: E731
+    y = np.zeros(a.rows)
+    for _ in range(args.warmup):
+        run(y)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run(y)
+        times.append(time.perf_counter() - t0)
+    bytes_ = a.bytes_spmv(8)
+    ms = 1e3 * statistics.mean(times)
+    gbs = bytes_ / (ms * 1e-3) / 1e9
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(gbs, 3), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows": a.rows, "nnz": a.nnz,
+                   "alpha": 1.0, "beta": 0.0, "bytes_per_step": bytes_},
+        "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads,
+                         "kind": kind,
+                         "sample": "full matrix, one reference SpmvReference call per "
+                                   "nnz-balanced row block per thread"},
+        "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def cpu_baseline_sample(a, x):
+    """The reference's serial CPU SpMV (1 core) on a bounded row sample."""
+    from oracle import Reference, Restatement, build_oracle
+    rows = min(a.rows, 1_048_576)
+    nnz = int(a.ptr[rows])
+    ptr, idx, val = a.ptr[:rows + 1], a.idx[:nnz], a.val[:nnz]
+    y = np.zeros(rows)
+    if Reference.available():
+        ref, kind = Reference(), "reference"
+        run = lambda: ref.compat_spmv(rows, a.cols, ptr, idx, val, 1.0, x, 0.0, y)  # noqa
+    else:
+        build_oracle.build_restatement()
+        rs, kind = Restatement(), "port"
+        run = lambda: rs.compat_spmv(ptr, idx, val, 1.0, x, 0.0, y)  # noqa
+    run()
+    times = []
+    t_end = time.perf_counter() + 10.0
+    while time.perf_counter() < t_end and len(times) < 20:
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    bytes_ = nnz * 16 + (rows + 1) * 8 + a.cols * 8 + rows * 8
+    gbs = bytes_ / statistics.median(times) / 1e9
+    return {"value": round(gbs, 4), "unit": "GB/s", "cores": 1, "kind": kind,
+            "sample": f"first {rows} rows ({nnz} nnz), median of {len(times)} calls"}
+
+
+def run_gpu(args, rank, world):
+    import torch
+    import torch.distributed as dist
+    from asc_cpp_b200 import _abi
+    from asc_cpp_b200.sparse_cuda import (CsrPlan, CudaCsrSpmv, CudaCsrSpmvWorkspaceSize,
+                                          CudaCsrArray, CudaStridedVectorView,
+                                          SparseCudaContext)
+    from asc_cpp_b200._abi import Determinism, Variant
+
+    local = _env_int("LOCAL_RANK", 0)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    a_h, x_h = _matrix()
+    stream = torch.cuda.Stream(device=dev)
+    ctx = SparseCudaContext.Create(local, stream=stream, determinism=Determinism.kDeterministic)
+    with torch.cuda.stream(stream):
+        A = CudaCsrArray(a_h.rows, a_h.cols, torch.from_numpy(a_h.ptr).to(dev),
+                         torch.from_numpy(a_h.idx).to(dev), torch.from_numpy(a_h.val).to(dev))
+        x = torch.from_numpy(x_h).to(dev)
+        y = torch.zeros(a_h.rows, dtype=torch.float64, device=dev)
+    stream.synchronize()
+    xv = CudaStridedVectorView(x, a_h.cols, writable=False)
+    yv = CudaStridedVectorView(y, a_h.rows)
+    bytes_step = a_h.bytes_spmv(8)
+
+    def timed(fn, steps, warmup):
+        for _ in range(warmup):
+            fn()
+        stream.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            fn()
+        stop.record(stream)
+        stop.synchronize()
+        torch.cuda.synchronize()
+        ms = start.elapsed_time(stop) / steps
+        if world > 1:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    # -- variants (untimed selection pass, then the headline) --
+    plan = CsrPlan(ctx, A)
+    detail = {}
+
+    def run_plan():
+        plan.csr_spmv(1.0, xv, 0.0, yv)
+
+    ctx.set_determinism(Determinism.kDeterministic)
+    detail["row_ordered_bitexact"] = bytes_step / (timed(run_plan, 5, 2) * 1e-3) / 1e9
+    ctx.set_determinism(Determinism.kBackendDefault)
+    for lanes in (2, 4, 8, 16):
+        ctx.set_variant(Variant.kVector, lanes)
+        detail[f"vector_{lanes}"] = bytes_step / (timed(run_plan, 5, 2) * 1e-3) / 1e9
+    best = max(detail, key=detail.get)
+    if best == "row_ordered_bitexact":
+        ctx.set_determinism(Determinism.kDeterministic)
+        mode = "deterministic (bit-exact row-ordered)"
+    else:
+        ctx.set_determinism(Determinism.kBackendDefault)
+        ctx.set_variant(Variant.kVector, int(best.split("_")[1]))
+        mode = f"backend_default ({best})"
+
+    # -- headline: device-resident inputs --
+    launches0 = ctx.launch_count
+    with Clocks(local) as clk:
+        ms = timed(run_plan, args.steps, args.warmup)
+    launches = (ctx.launch_count - launches0) // (args.steps + args.warmup)
+    gbs = bytes_step / (ms * 1e-3) / 1e9
+
+    # -- end to end through the C ABI with host buffers --
+    x_pin = torch.from_numpy(x_h).pin_memory()
+    y_pin = torch.empty(a_h.rows, dtype=torch.float64).pin_memory()
+    ws_bytes = CudaCsrSpmvWorkspaceSize(ctx, A, xv, yv)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+
+    def run_e2e():
+        with torch.cuda.stream(stream):
+            x.copy_(x_pin, non_blocking=True)
+            CudaCsrSpmv(ctx, 1.0, A, xv, 0.0, yv, ws, ws_bytes)
+            y_pin.copy_(y, non_blocking=True)
+
+    e2e_ms = timed(run_e2e, max(3, args.steps // 2), 2)
+    e2e_gbs = bytes_step / (e2e_ms * 1e-3) / 1e9
+
+    # correctness of the last result against the oracle (rows sample)
+    stream.synchronize()
+    peak, peak_kind = _peaks()
+    traffic = _traffic_record().get(WORKLOAD)
+    out = None
+    if rank == 0:
+        cpu = cpu_baseline_sample(a_h, x_h) if world == 1 else None
+        out = {
+            "metric": METRIC, "value": round(gbs * world, 3), "unit": "GB/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows": a_h.rows, "nnz": a_h.nnz,
+                       "alpha": 1.0, "beta": 0.0, "bytes_per_step": bytes_step,
+                       "l2": "inputs (1.18 GB) larger than L2; no flush",
+                       "mode": mode, "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 2), "peak": peak,
+                         "unit": "GB/s", "frac": round(gbs / peak, 4),
+                         "traffic": traffic, "peak_kind": peak_kind},
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_gbs * world, 3), "unit": "GB/s",
+                    "h2d_bytes_per_step": a_h.cols * 8, "d2h_bytes_per_step": a_h.rows * 8,
+                    "ms_per_step": round(e2e_ms, 4),
+                    "note": "A cloned to HBM once (CudaCloneCsr); x H2D and y D2H every step"},
+            "gpu_launches": int(launches * args.steps),
+            "clocks": clk.summary(),
+            "detail_gbs": {k: round(v, 2) for k, v in detail.items()},
+        }
+    plan.close()
+    ctx.close()
+    return out
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    args = p.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = _env_int("RANK", 0)
+    world = _env_int("WORLD_SIZE", 1)
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    import torch.distributed as dist
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    try:
+        out = run_gpu(args, rank, world)
+        if out is not None:
+            print(json.dumps(out), flush=True)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

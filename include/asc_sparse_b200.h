@@ -1,0 +1,256 @@
+/*
+ * asc_sparse_b200.h - C ABI of the B200-native Sparse BLAS hot path.
+ *
+ * This library replaces the computational back end of ASCCpp's experimental
+ * `sparse_cuda` provider facet (reference: include/asc/sparse/providers/
+ * cuda.h, src/sparse/cuda/operations.cc, src/sparse/cuda/kernels.cu).  Every
+ * entry point takes plain pointers, sizes and enums -- no C++ or torch types --
+ * so that the reference's exported `internal_sparse_cuda::*Erased` functions
+ * can forward to it one-for-one, and so that ctypes,
+ * cgo or any other FFI can bind it directly.
+ *
+ * Semantics mirror the reference exactly:
+ *   - enum values are numerically identical to the reference enums;
+ *   - status codes are the reference's asc::ErrorCode values
+ *     (include/asc/core/status.h:35-55);
+ *   - every call validates completely before it enqueues anything, so a
+ *     failing call never writes an output (operations.cc:349-398);
+ *   - work is enqueued on the context's stream; success never implies a host
+ *     wait (docs/modules/sparse.md:441-442);
+ *   - a failure detected after enqueue synchronizes the stream before it
+ *     returns (operations.cc:1027-1045).
+ * All kernels are hand-written for sm_100a; there is no cuSPARSE, cuBLAS or
+ * CPU fallback behind any entry point.
+ */
+#ifndef ASC_SPARSE_B200_H_
+#define ASC_SPARSE_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(_WIN32)
+#define ASC_SB_API __declspec(dllexport)
+#else
+#define ASC_SB_API __attribute__((visibility("default")))
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- enums (values identical to the reference) --------------------------- */
+
+/* asc::ErrorCode, include/asc/core/status.h:35-55 */
+typedef enum asc_sb_status {
+  ASC_SB_OK = 0,
+  ASC_SB_INVALID_ARGUMENT = 1,
+  ASC_SB_SHAPE = 2,
+  ASC_SB_INDEX = 3,
+  ASC_SB_OVERFLOW = 4,
+  ASC_SB_INVALID_STATE = 5,
+  ASC_SB_ALLOCATION = 6,
+  ASC_SB_MEMORY_ACCESS = 7,
+  ASC_SB_MEMORY_TRANSFER = 8,
+  ASC_SB_UNSUPPORTED = 9,
+  ASC_SB_UNAVAILABLE = 10,
+  ASC_SB_PROVIDER = 11,
+  ASC_SB_NUMERICAL = 12,
+  ASC_SB_INTERNAL = 18
+} asc_sb_status;
+
+/* asc::MemorySpace, include/asc/core/memory.h:30-35 */
+enum { ASC_SB_HOST = 0, ASC_SB_PINNED_HOST = 1, ASC_SB_DEVICE = 2,
+       ASC_SB_MANAGED = 3 };
+
+/* internal_sparse_cuda::ElementKind, include/asc/sparse/providers/cuda.h:103-108 */
+enum { ASC_SB_FLOAT = 0, ASC_SB_DOUBLE = 1, ASC_SB_COMPLEX_FLOAT = 2,
+       ASC_SB_COMPLEX_DOUBLE = 3 };
+
+/* internal_sparse_cuda::FormatKind, cuda.h:123-127 */
+enum { ASC_SB_COORDINATE = 0, ASC_SB_CSR = 1, ASC_SB_CSC = 2 };
+
+/* asc::SparseBlasTranspose, include/asc/sparse/blas.h:88-92 */
+enum { ASC_SB_OP_NONE = 0, ASC_SB_OP_TRANSPOSE = 1,
+       ASC_SB_OP_CONJUGATE_TRANSPOSE = 2 };
+
+/* asc::SparseBlasLayout, include/asc/sparse/blas.h:103-106 */
+enum { ASC_SB_COLUMN_MAJOR = 0, ASC_SB_ROW_MAJOR = 1 };
+
+/* asc::Determinism, include/asc/core/execution.h:122-125.  DETERMINISTIC (the
+ * reference's default) runs the row-ordered kernels, which reproduce the
+ * reference's serial summation order and rounding bit for bit.
+ * BACKEND_DEFAULT lets the library pick the fastest variant, whose results
+ * stay within |y - y_ref| <= gamma_{n+2} * (|alpha| |A| |x| + |beta| |y|),
+ * gamma_k = k u / (1 - k u), n = stored entries of the row. */
+enum { ASC_SB_DETERMINISTIC = 0, ASC_SB_BACKEND_DEFAULT = 1 };
+
+/* SpMV kernel variants (no reference counterpart; the reference has one
+ * thread-per-row kernel, src/sparse/cuda/kernels.cu:91-115). */
+enum {
+  ASC_SB_VARIANT_AUTO = -1,      /* library choice (selector / heuristics) */
+  ASC_SB_VARIANT_ROW_ORDERED = 0,/* bit-exact serial order, CTA row tiles   */
+  ASC_SB_VARIANT_VECTOR = 1,     /* 'lanes' threads per row, shuffle sums   */
+  ASC_SB_VARIANT_MERGE_PATH = 2, /* merge-path balanced tiles + fix-up      */
+  ASC_SB_VARIANT_ROW_SPLIT = 3   /* vector rows + long rows split over CTAs */
+};
+
+/* ---- descriptors ---------------------------------------------------------- */
+
+/* internal_sparse_cuda::SparseDescriptor, cuda.h:143-156 (rank fixed at two).
+ * CSR: structure_first = int64 outer offsets [rows+1],
+ *      structure_second = int64 column indices [nonzeros].
+ * CSC: outer offsets over columns [columns+1], row indices [nonzeros].
+ * Structure must be canonical (zero based, sorted, unique) and the caller
+ * asserts that by setting canonical_structure_trusted, exactly as the
+ * reference's trusted device clones do (compressed.h:759-770). */
+typedef struct asc_sb_sparse {
+  const void* structure_first;
+  const void* structure_second;
+  const void* values;
+  int32_t memory_space;
+  int32_t element_kind;
+  int32_t format;
+  int32_t canonical_structure_trusted;
+  int64_t rows;
+  int64_t columns;
+  int64_t nonzeros;
+} asc_sb_sparse;
+
+/* internal_sparse_cuda::VectorDescriptor, cuda.h:164-173.  Element i is at
+ * data[i * stride]; for a negative stride `data` is logical element 0 and
+ * reachable_data/reachable_size (optional) give the backing span. */
+typedef struct asc_sb_vector {
+  const void* data;
+  const void* reachable_data;
+  size_t reachable_size;
+  int32_t memory_space;
+  int32_t element_kind;
+  int64_t extent;
+  int64_t stride;
+  int32_t writable;
+  int32_t reserved;
+} asc_sb_vector;
+
+/* internal_sparse_cuda::MatrixDescriptor, cuda.h:186-197. */
+typedef struct asc_sb_dense {
+  const void* data;
+  const void* reachable_data;
+  size_t reachable_size;
+  int32_t memory_space;
+  int32_t element_kind;
+  int64_t rows;
+  int64_t columns;
+  int64_t leading_dimension;
+  int32_t layout;
+  int32_t writable;
+} asc_sb_dense;
+
+typedef struct asc_sb_context asc_sb_context;
+
+/* ---- context -------------------------------------------------------------- */
+
+/* Replaces SparseCudaContext::Create (cuda.h:514; src/sparse/cuda/context.cc:
+ * 69-113).  `stream` is a cudaStream_t on `device` (the reference passes the
+ * ExecutionContext's native stream, src/core/cuda/runtime.cc:454; the legacy
+ * default stream is cudaStreamLegacy, (void*)0x1); NULL makes the context
+ * create and own a non-blocking stream.  Determinism starts at
+ * ASC_SB_DETERMINISTIC, the reference default (execution.h:162). */
+ASC_SB_API int asc_sb_context_create(int32_t device, void* stream,
+                                     asc_sb_context** out);
+/* Replaces ~SparseCudaContext (cuda.h:588). NULL is accepted. */
+ASC_SB_API int asc_sb_context_destroy(asc_sb_context* context);
+ASC_SB_API int asc_sb_context_set_determinism(asc_sb_context* context,
+                                              int32_t determinism);
+/* Forces one SpMV variant (for autotuning and tests).  `lanes` is the threads
+ * per row of the VECTOR / ROW_SPLIT variants (1..32, power of two; 0 = auto). */
+ASC_SB_API int asc_sb_context_set_variant(asc_sb_context* context,
+                                          int32_t variant, int32_t lanes);
+ASC_SB_API void* asc_sb_context_stream(const asc_sb_context* context);
+ASC_SB_API int asc_sb_context_synchronize(asc_sb_context* context);
+/* Message of the most recent failure on this context ("" if none). */
+ASC_SB_API const char* asc_sb_context_last_error(const asc_sb_context* context);
+/* Kernel launches issued by this context since creation (instrumentation). */
+ASC_SB_API int64_t asc_sb_context_launch_count(const asc_sb_context* context);
+
+/* ---- compat SpMV  y = alpha * A * x + beta * y ----------------------------- */
+
+/* Replaces internal_sparse_cuda::CsrSpmvWorkspaceSizeErased (cuda.h:220-222;
+ * operations.cc:884-909).  The size is stable for a given (A, x, y) shape. */
+ASC_SB_API int asc_sb_csr_spmv_workspace_size(asc_sb_context* context,
+                                              const asc_sb_sparse* matrix,
+                                              const asc_sb_vector* input,
+                                              const asc_sb_vector* output,
+                                              size_t* bytes);
+
+/* Replaces internal_sparse_cuda::CsrSpmvErased (cuda.h:224-227;
+ * operations.cc:911-1049) and the compat path it serves
+ * (SpmvReferenceImpl, src/sparse/reference_blas.cc:9-41).  alpha and beta
+ * arrive as double for both element kinds and are rounded to the element type
+ * (operations.cc:1010-1013).  beta == 0 never reads y.  `workspace` must be
+ * device memory of at least the queried size (or NULL/0 when that size is 0),
+ * 256-byte aligned and disjoint from every operand. */
+ASC_SB_API int asc_sb_csr_spmv(asc_sb_context* context, double alpha,
+                               const asc_sb_sparse* matrix,
+                               const asc_sb_vector* input, double beta,
+                               const asc_sb_vector* output, void* workspace,
+                               size_t workspace_bytes,
+                               int32_t workspace_space);
+
+/* ---- standard SpMV / SpMM  y += alpha * op(A) * x -------------------------- */
+
+/* Replaces internal_sparse_cuda::StandardSpmvErased (cuda.h:243-246;
+ * operations.cc:1214-1299) and the CPU template it must agree with
+ * (blas.h:1607-1667).  alpha_imag must be 0 (real element kinds).  CSR and
+ * CSC are both accepted: CSC with op = none is computed as the transpose of
+ * the CSR matrix with the same arrays.  A transpose (of CSR) in
+ * DETERMINISTIC mode needs the transposed structure, which lives in a plan
+ * (asc_sb_plan_create); without one the call returns ASC_SB_INVALID_STATE. */
+ASC_SB_API int asc_sb_standard_spmv(asc_sb_context* context, int32_t op,
+                                    double alpha_real, double alpha_imag,
+                                    const asc_sb_sparse* matrix,
+                                    const asc_sb_vector* input,
+                                    const asc_sb_vector* output);
+
+/* Replaces internal_sparse_cuda::StandardSpmmErased (cuda.h:248-251;
+ * operations.cc:1301-1378), CPU contract blas.h:1692-1750. */
+ASC_SB_API int asc_sb_standard_spmm(asc_sb_context* context, int32_t op,
+                                    double alpha_real, double alpha_imag,
+                                    const asc_sb_sparse* matrix,
+                                    const asc_sb_dense* input,
+                                    const asc_sb_dense* output);
+
+/* ---- analysis plans (no reference counterpart) ----------------------------
+ * A plan caches, in caller-provided device memory, everything the kernels can
+ * reuse across calls on one matrix: the row-tile and merge-path partitions and
+ * (optionally) the transposed structure with its values.  The matrix's values
+ * must not change while a plan built with ASC_SB_PLAN_TRANSPOSE is in use
+ * (call asc_sb_plan_refresh_values after changing them). */
+enum { ASC_SB_PLAN_TRANSPOSE = 1 };
+typedef struct asc_sb_plan asc_sb_plan;
+ASC_SB_API int asc_sb_plan_workspace_size(asc_sb_context* context,
+                                          const asc_sb_sparse* matrix,
+                                          int32_t flags, size_t* bytes);
+ASC_SB_API int asc_sb_plan_create(asc_sb_context* context,
+                                  const asc_sb_sparse* matrix, int32_t flags,
+                                  void* workspace, size_t workspace_bytes,
+                                  asc_sb_plan** out);
+ASC_SB_API int asc_sb_plan_refresh_values(asc_sb_context* context,
+                                          asc_sb_plan* plan);
+ASC_SB_API int asc_sb_plan_destroy(asc_sb_plan* plan);
+/* Compat SpMV through a plan: same contract as asc_sb_csr_spmv. */
+ASC_SB_API int asc_sb_plan_csr_spmv(asc_sb_context* context,
+                                    const asc_sb_plan* plan, double alpha,
+                                    const asc_sb_vector* input, double beta,
+                                    const asc_sb_vector* output);
+/* Standard SpMV through a plan: same contract as asc_sb_standard_spmv. */
+ASC_SB_API int asc_sb_plan_standard_spmv(asc_sb_context* context,
+                                         const asc_sb_plan* plan, int32_t op,
+                                         double alpha_real, double alpha_imag,
+                                         const asc_sb_vector* input,
+                                         const asc_sb_vector* output);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* ASC_SPARSE_B200_H_ */

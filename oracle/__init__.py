@@ -1,0 +1,229 @@
+"""CPU oracle for the Sparse BLAS hot path -- test infrastructure only.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` may import this package, and only as the checker.  The product
+(``asc_cpp_b200``) never imports it.
+
+Two backends:
+
+* :class:`Restatement` - ``liboracle.so``, the C restatement in
+  ``sparse_oracle.c`` (always available once built).
+* :class:`Reference` - ``_ref/libasc_ref.so``, the reference's own serial
+  Sparse BLAS compiled from its sources (present where it could be built).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build_oracle
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_INT = ctypes.c_int
+_SZ = ctypes.c_size_t
+
+CSR, CSC = 1, 2
+OP_NONE, OP_TRANSPOSE, OP_CONJ_TRANSPOSE = 0, 1, 2
+COL_MAJOR, ROW_MAJOR = 0, 1
+
+
+def _ptr(a: np.ndarray | None) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+def _scalar(dtype):
+    return ctypes.c_double if np.dtype(dtype) == np.float64 else ctypes.c_float
+
+
+def _suffix(dtype) -> str:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return "f64"
+    if dt == np.float32:
+        return "f32"
+    raise TypeError(f"oracle supports float32/float64, not {dt}")
+
+
+class Restatement:
+    """ctypes front end of ``liboracle.so``."""
+
+    def __init__(self, path: str | None = None):
+        path = path or build_oracle.ORACLE_SO
+        if not os.path.exists(path):
+            build_oracle.build_restatement()
+        self.lib = ctypes.CDLL(path)
+        for sfx, sc in (("f64", ctypes.c_double), ("f32", ctypes.c_float)):
+            f = getattr(self.lib, f"oracle_compat_spmv_{sfx}")
+            f.restype = None
+            f.argtypes = [_I64, _P, _P, _P, sc, _P, _I64, sc, _P, _I64]
+            f = getattr(self.lib, f"oracle_standard_spmv_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, sc, _P, _I64, _P,
+                          _I64]
+            f = getattr(self.lib, f"oracle_standard_spmm_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, sc, _P, _INT, _I64,
+                          _P, _INT, _I64, _I64]
+            f = getattr(self.lib, f"oracle_csr_extended_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _I64, _I64, _P, _P, _P, _P, _P, _P]
+        self.lib.oracle_output_counts.restype = None
+        self.lib.oracle_output_counts.argtypes = [_INT, _I64, _I64, _P, _P, _P]
+        self.lib.oracle_csr_transpose_structure.restype = None
+        self.lib.oracle_csr_transpose_structure.argtypes = [_I64, _I64, _P, _P,
+                                                            _P, _P, _P]
+        self.lib.oracle_merge_path_split.restype = None
+        self.lib.oracle_merge_path_split.argtypes = [
+            _I64, _P, _I64, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]
+
+    # -- compat y = alpha*A*x + beta*y (strided; x, y point at element 0) --
+    def compat_spmv(self, ptr, idx, val, alpha, x, beta, y, incx=1, incy=1):
+        rows = len(ptr) - 1
+        sc = _scalar(val.dtype)
+        getattr(self.lib, f"oracle_compat_spmv_{_suffix(val.dtype)}")(
+            rows, _ptr(ptr), _ptr(idx), _ptr(val), sc(alpha), _ptr(x), incx,
+            sc(beta), _ptr(y), incy)
+        return y
+
+    def standard_spmv(self, fmt, op, rows, cols, ptr, idx, val, alpha, x, y,
+                      incx=1, incy=1, x_offset=0, y_offset=0):
+        """y += alpha*op(A)*x; ``*_offset`` = element index of logical 0."""
+        sc = _scalar(val.dtype)
+        xs = x.ctypes.data + x_offset * x.itemsize
+        ys = y.ctypes.data + y_offset * y.itemsize
+        getattr(self.lib, f"oracle_standard_spmv_{_suffix(val.dtype)}")(
+            fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), sc(alpha), xs,
+            incx, ys, incy)
+        return y
+
+    def standard_spmm(self, fmt, op, rows, cols, ptr, idx, val, alpha, b,
+                      b_layout, ldb, c, c_layout, ldc, ncols):
+        sc = _scalar(val.dtype)
+        getattr(self.lib, f"oracle_standard_spmm_{_suffix(val.dtype)}")(
+            fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), sc(alpha),
+            _ptr(b), b_layout, ldb, _ptr(c), c_layout, ldc, ncols)
+        return c
+
+    def extended(self, op, rows, cols, ptr, idx, val, x):
+        """(exact sum, sum of |products|) per output of op(A)x, long double."""
+        n_out = rows if op == OP_NONE else cols
+        exact = np.zeros(n_out, dtype=np.longdouble)
+        absval = np.zeros(n_out, dtype=np.longdouble)
+        getattr(self.lib, f"oracle_csr_extended_{_suffix(val.dtype)}")(
+            op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), _ptr(x),
+            _ptr(exact), _ptr(absval))
+        return exact, absval
+
+    def output_counts(self, op, rows, cols, ptr, idx):
+        n_out = rows if op == OP_NONE else cols
+        counts = np.zeros(n_out, dtype=np.int64)
+        self.lib.oracle_output_counts(op, rows, cols, _ptr(ptr), _ptr(idx),
+                                      _ptr(counts))
+        return counts
+
+    def transpose_structure(self, rows, cols, ptr, idx):
+        nnz = int(ptr[rows])
+        t_ptr = np.zeros(cols + 1, dtype=np.int64)
+        t_idx = np.zeros(max(nnz, 1), dtype=np.int64)
+        perm = np.zeros(max(nnz, 1), dtype=np.int64)
+        self.lib.oracle_csr_transpose_structure(rows, cols, _ptr(ptr),
+                                                _ptr(idx), _ptr(t_ptr),
+                                                _ptr(t_idx), _ptr(perm))
+        return t_ptr, t_idx[:nnz], perm[:nnz]
+
+    def merge_path_split(self, ptr, diagonal):
+        rows = len(ptr) - 1
+        r = _I64()
+        z = _I64()
+        self.lib.oracle_merge_path_split(rows, _ptr(ptr), int(ptr[-1]),
+                                         int(diagonal), ctypes.byref(r),
+                                         ctypes.byref(z))
+        return r.value, z.value
+
+
+class Reference:
+    """ctypes front end of the reference's own serial Sparse BLAS."""
+
+    def __init__(self, path: str | None = None):
+        path = path or build_oracle.REF_SO
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = ctypes.CDLL(path)
+        for sfx, sc in (("f64", ctypes.c_double), ("f32", ctypes.c_float)):
+            f = getattr(self.lib, f"ref_compat_spmv_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_I64, _I64, _P, _P, _P, _I64, sc, _P, _I64, sc, _P,
+                          _I64]
+            f = getattr(self.lib, f"ref_standard_spmv_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, _I64, sc, _P, _I64,
+                          _I64, _SZ, _P, _I64, _I64, _SZ]
+            f = getattr(self.lib, f"ref_standard_spmm_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, _I64, sc, _P, _I64,
+                          _I64, _INT, _I64, _SZ, _P, _I64, _I64, _INT, _I64, _SZ]
+            f = getattr(self.lib, f"ref_blocks_prepare_{sfx}")
+            f.restype = _P
+            f.argtypes = [_I64, _I64, _P, _P, _P, _INT]
+            f = getattr(self.lib, f"ref_blocks_run_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_P, sc, _P, sc, _P]
+            f = getattr(self.lib, f"ref_blocks_free_{sfx}")
+            f.restype = None
+            f.argtypes = [_P]
+
+    @staticmethod
+    def available() -> bool:
+        return os.path.exists(build_oracle.REF_SO)
+
+    def compat_spmv(self, rows, cols, ptr, idx, val, alpha, x, beta, y,
+                    incx=1, incy=1) -> int:
+        sc = _scalar(val.dtype)
+        return getattr(self.lib, f"ref_compat_spmv_{_suffix(val.dtype)}")(
+            rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), int(ptr[rows]),
+            sc(alpha), _ptr(x), incx, sc(beta), _ptr(y), incy)
+
+    def standard_spmv(self, fmt, op, rows, cols, ptr, idx, val, alpha, x, y,
+                      incx=1, incy=1, x_offset=0, y_offset=0) -> int:
+        sc = _scalar(val.dtype)
+        outer = rows if fmt == CSR else cols
+        nx = cols if op == OP_NONE else rows
+        ny = rows if op == OP_NONE else cols
+        xs = x.ctypes.data + x_offset * x.itemsize
+        ys = y.ctypes.data + y_offset * y.itemsize
+        return getattr(self.lib, f"ref_standard_spmv_{_suffix(val.dtype)}")(
+            fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val),
+            int(ptr[outer]), sc(alpha), xs, nx, incx, x.size, ys, ny, incy,
+            y.size)
+
+    def standard_spmm(self, fmt, op, rows, cols, ptr, idx, val, alpha, b,
+                      b_rows, b_cols, b_layout, ldb, c, c_rows, c_cols,
+                      c_layout, ldc) -> int:
+        sc = _scalar(val.dtype)
+        outer = rows if fmt == CSR else cols
+        return getattr(self.lib, f"ref_standard_spmm_{_suffix(val.dtype)}")(
+            fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val),
+            int(ptr[outer]), sc(alpha), _ptr(b), b_rows, b_cols, b_layout, ldb,
+            b.size, _ptr(c), c_rows, c_cols, c_layout, ldc, c.size)
+
+    # row-block parallel compat SpMV (each block is the reference's serial
+    # SpmvReference on a disjoint row range)
+    def blocks_prepare(self, rows, cols, ptr, idx, val, nblocks):
+        h = getattr(self.lib, f"ref_blocks_prepare_{_suffix(val.dtype)}")(
+            rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), nblocks)
+        if not h:
+            raise RuntimeError("reference rejected a row block")
+        return h
+
+    def blocks_run(self, h, dtype, alpha, x, beta, y) -> int:
+        sc = _scalar(dtype)
+        return getattr(self.lib, f"ref_blocks_run_{_suffix(dtype)}")(
+            h, sc(alpha), _ptr(x), sc(beta), _ptr(y))
+
+    def blocks_free(self, h, dtype) -> None:
+        getattr(self.lib, f"ref_blocks_free_{_suffix(dtype)}")(h)

@@ -1,0 +1,225 @@
+/*
+ * CPU oracle for the Sparse BLAS hot path -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C restatement of the reference's serial algorithms, used by tests/,
+ * by __graft_entry__.smoke() and by bench.py's CPU-baseline leg as the checker.
+ * The product path never links, loads or calls this file.
+ *
+ * Parity of this restatement is pinned two ways (tests/test_oracle.py):
+ *   1. bit-exact agreement with oracle/_ref/libasc_ref.so, the reference's own
+ *      sources compiled unchanged, on seeded random inputs, and
+ *   2. the known-answer vectors of the reference's tests, stored as fixtures
+ *      under tests/golden/ together with the script that generated them.
+ *
+ * Floating point: compiled with -O2 -ffp-contract=off and no -march flag, the
+ * same as the reference's x86-64 build, so every * and + rounds separately and
+ * no fused multiply-add appears.
+ *
+ * Layout conventions (the reference's, include/asc/core/types.h:35,62):
+ *   CSR: ptr[rows+1], idx[nnz] (column per entry), val[nnz]; int64 indices.
+ *   CSC: ptr[cols+1], idx[nnz] (row per entry),    val[nnz].
+ *   Vectors: logical element i lives at x[i * inc]; inc may be negative, in
+ *   which case x points at logical element 0 (include/asc/sparse/blas.h:1277).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+enum { ORACLE_CSR = 1, ORACLE_CSC = 2 };
+enum { ORACLE_OP_NONE = 0, ORACLE_OP_TRANSPOSE = 1, ORACLE_OP_CONJ_TRANSPOSE = 2 };
+enum { ORACLE_COL_MAJOR = 0, ORACLE_ROW_MAJOR = 1 };
+
+/* ------------------------------------------------------------------------- */
+/* Compat SpMV y = alpha * (sum_k v_k x_{c_k}) + beta * y.
+ * Restates SpmvReferenceImpl, src/sparse/reference_blas.cc:9-41:
+ *   product starts at Element{} (+0.0) and accumulates value * x[col] in
+ *   stored order; result = alpha * product; if beta != 0 then
+ *   result += beta * y_old (beta == 0 never reads y); write result.        */
+#define ORACLE_COMPAT(SUFFIX, T)                                               \
+  void oracle_compat_spmv_##SUFFIX(int64_t rows, const int64_t* ptr,           \
+                                   const int64_t* idx, const T* val, T alpha,  \
+                                   const T* x, int64_t incx, T beta, T* y,     \
+                                   int64_t incy) {                             \
+    for (int64_t r = 0; r < rows; ++r) {                                       \
+      T product = (T)0;                                                        \
+      for (int64_t p = ptr[r]; p < ptr[r + 1]; ++p) {                          \
+        product += val[p] * x[idx[p] * incx];                                  \
+      }                                                                        \
+      T result = alpha * product;                                              \
+      if (beta != (T)0) {                                                      \
+        result += beta * y[r * incy];                                          \
+      }                                                                        \
+      y[r * incy] = result;                                                    \
+    }                                                                          \
+  }
+ORACLE_COMPAT(f64, double)
+ORACLE_COMPAT(f32, float)
+
+/* ------------------------------------------------------------------------- */
+/* Standard SpMV y += alpha * op(A) * x.
+ * Restates asc::Spmv, include/asc/sparse/blas.h:1607-1667 with ForEachStored
+ * (:1241-1256): alpha == 0 returns without touching y; otherwise the stored
+ * entries are visited outer index ascending, then stored position ascending,
+ * and each does y[out] += alpha * value * x[in] -- evaluated left to right,
+ * i.e. (alpha * value) * x[in], then added to y[out].  For CSR outer = row,
+ * for CSC outer = column; op != none swaps out and in.  Real types only, so
+ * the conjugate transpose equals the transpose.                             */
+#define ORACLE_STANDARD_SPMV(SUFFIX, T)                                        \
+  void oracle_standard_spmv_##SUFFIX(int format, int op, int64_t rows,         \
+                                     int64_t cols, const int64_t* ptr,         \
+                                     const int64_t* idx, const T* val,         \
+                                     T alpha, const T* x, int64_t incx, T* y,  \
+                                     int64_t incy) {                           \
+    if (alpha == (T)0) return;                                                 \
+    const int64_t outer_extent = format == ORACLE_CSC ? cols : rows;           \
+    for (int64_t o = 0; o < outer_extent; ++o) {                               \
+      for (int64_t p = ptr[o]; p < ptr[o + 1]; ++p) {                         \
+        int64_t row = format == ORACLE_CSC ? idx[p] : o;                       \
+        int64_t col = format == ORACLE_CSC ? o : idx[p];                       \
+        int64_t out = row, in = col;                                           \
+        if (op != ORACLE_OP_NONE) {                                            \
+          out = col;                                                           \
+          in = row;                                                            \
+        }                                                                      \
+        y[out * incy] += alpha * val[p] * x[in * incx];                        \
+      }                                                                        \
+    }                                                                          \
+  }
+ORACLE_STANDARD_SPMV(f64, double)
+ORACLE_STANDARD_SPMV(f32, float)
+
+/* ------------------------------------------------------------------------- */
+/* Standard SpMM C += alpha * op(A) * B.
+ * Restates asc::Spmm, include/asc/sparse/blas.h:1692-1750: same entry order as
+ * SpMV, with an inner loop over the right-hand sides j = 0..ncols-1 doing
+ * C(out, j) += alpha * value * B(in, j).  Element (r, c) of a dense matrix is
+ * at r*ld + c (row major) or c*ld + r (column major), blas.h:1033-1038.     */
+static inline int64_t dense_at(int layout, int64_t ld, int64_t r, int64_t c) {
+  return layout == ORACLE_ROW_MAJOR ? r * ld + c : c * ld + r;
+}
+#define ORACLE_STANDARD_SPMM(SUFFIX, T)                                        \
+  void oracle_standard_spmm_##SUFFIX(                                          \
+      int format, int op, int64_t rows, int64_t cols, const int64_t* ptr,      \
+      const int64_t* idx, const T* val, T alpha, const T* b, int b_layout,     \
+      int64_t ldb, T* c, int c_layout, int64_t ldc, int64_t ncols) {           \
+    if (alpha == (T)0) return;                                                 \
+    const int64_t outer_extent = format == ORACLE_CSC ? cols : rows;           \
+    for (int64_t o = 0; o < outer_extent; ++o) {                               \
+      for (int64_t p = ptr[o]; p < ptr[o + 1]; ++p) {                         \
+        int64_t row = format == ORACLE_CSC ? idx[p] : o;                       \
+        int64_t col = format == ORACLE_CSC ? o : idx[p];                       \
+        int64_t out = row, in = col;                                           \
+        if (op != ORACLE_OP_NONE) {                                            \
+          out = col;                                                           \
+          in = row;                                                            \
+        }                                                                      \
+        for (int64_t j = 0; j < ncols; ++j) {                                  \
+          c[dense_at(c_layout, ldc, out, j)] +=                                \
+              alpha * val[p] * b[dense_at(b_layout, ldb, in, j)];              \
+        }                                                                      \
+      }                                                                        \
+    }                                                                          \
+  }
+ORACLE_STANDARD_SPMM(f64, double)
+ORACLE_STANDARD_SPMM(f32, float)
+
+/* ------------------------------------------------------------------------- */
+/* Extended-precision companions used to state and check error bounds.
+ * For each output o of op(A) (CSR, unit-stride vectors) they return
+ *   exact[o] ~= sum_k v_k x_k   (long double accumulation of exact products)
+ *   absval[o] = sum_k |v_k| |x_k|
+ * so that a result r can be checked against |r - exact| <= g * absval.     */
+#define ORACLE_EXTENDED(SUFFIX, T)                                             \
+  void oracle_csr_extended_##SUFFIX(int op, int64_t rows, int64_t cols,        \
+                                    const int64_t* ptr, const int64_t* idx,    \
+                                    const T* val, const T* x,                  \
+                                    long double* exact, long double* absval) { \
+    const int64_t n_out = op == ORACLE_OP_NONE ? rows : cols;                  \
+    for (int64_t o = 0; o < n_out; ++o) {                                      \
+      exact[o] = 0.0L;                                                         \
+      absval[o] = 0.0L;                                                        \
+    }                                                                          \
+    for (int64_t r = 0; r < rows; ++r) {                                       \
+      for (int64_t p = ptr[r]; p < ptr[r + 1]; ++p) {                         \
+        const int64_t out = op == ORACLE_OP_NONE ? r : idx[p];                 \
+        const int64_t in = op == ORACLE_OP_NONE ? idx[p] : r;                  \
+        const long double prod = (long double)val[p] * (long double)x[in];     \
+        exact[out] += prod;                                                    \
+        absval[out] += fabsl(prod);                                            \
+      }                                                                        \
+    }                                                                          \
+  }
+ORACLE_EXTENDED(f64, double)
+ORACLE_EXTENDED(f32, float)
+
+/* Row lengths of op(A): the n in gamma_n for each output. */
+void oracle_output_counts(int op, int64_t rows, int64_t cols,
+                          const int64_t* ptr, const int64_t* idx,
+                          int64_t* counts) {
+  const int64_t n_out = op == ORACLE_OP_NONE ? rows : cols;
+  memset(counts, 0, (size_t)n_out * sizeof(int64_t));
+  for (int64_t r = 0; r < rows; ++r) {
+    if (op == ORACLE_OP_NONE) {
+      counts[r] = ptr[r + 1] - ptr[r];
+    } else {
+      for (int64_t p = ptr[r]; p < ptr[r + 1]; ++p) counts[idx[p]] += 1;
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* CSR -> CSC (equivalently: the CSR structure of A^T), integer work.
+ * Restates the column-major re-compression of
+ * CompressedSparseArray::FromCompressed, include/asc/sparse/compressed.h:
+ * 1151-1221: entries of each output column appear in increasing source row,
+ * which is exactly the order the standard transpose visits them
+ * (blas.h:1241-1256).  perm[q] = source position of transposed entry q.     */
+void oracle_csr_transpose_structure(int64_t rows, int64_t cols,
+                                    const int64_t* ptr, const int64_t* idx,
+                                    int64_t* t_ptr, int64_t* t_idx,
+                                    int64_t* perm) {
+  memset(t_ptr, 0, (size_t)(cols + 1) * sizeof(int64_t));
+  const int64_t nnz = ptr[rows];
+  for (int64_t p = 0; p < nnz; ++p) t_ptr[idx[p] + 1] += 1;
+  for (int64_t c = 0; c < cols; ++c) t_ptr[c + 1] += t_ptr[c];
+  int64_t* next = (int64_t*)malloc((size_t)(cols > 0 ? cols : 1) * sizeof(int64_t));
+  if (next == NULL) return;
+  memcpy(next, t_ptr, (size_t)cols * sizeof(int64_t));
+  for (int64_t r = 0; r < rows; ++r) {
+    for (int64_t p = ptr[r]; p < ptr[r + 1]; ++p) {
+      const int64_t q = next[idx[p]]++;
+      t_idx[q] = r;
+      perm[q] = p;
+    }
+  }
+  free(next);
+}
+
+/* ------------------------------------------------------------------------- */
+/* Merge-path split of the (row-end, nonzero) merge of a CSR matrix.
+ * The merge interleaves list A = ptr[1..rows] (the end offset of each row)
+ * with list B = 0, 1, ..., nnz-1 (the nonzero positions), taking a nonzero
+ * while its position is below the current row's end.  Diagonal d of the
+ * merge grid is split at (i, d - i): i row ends and d - i nonzeros consumed.
+ * i is found by binary search as the first candidate in
+ * [max(0, d - nnz), min(d, rows)] with A[i] > B[d - i - 1]
+ * (Odeh et al., "Merge Path", 2012; applied to CSR SpMV by Merrill and
+ * Garland, 2016).  The reference has no counterpart; the GPU partition kernel
+ * must reproduce these integers exactly.                                    */
+void oracle_merge_path_split(int64_t rows, const int64_t* ptr, int64_t nnz,
+                             int64_t diagonal, int64_t* row_out,
+                             int64_t* nz_out) {
+  int64_t lo = diagonal - nnz > 0 ? diagonal - nnz : 0;
+  int64_t hi = diagonal < rows ? diagonal : rows;
+  while (lo < hi) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (ptr[mid + 1] <= diagonal - mid - 1) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  *row_out = lo;
+  *nz_out = diagonal - lo;
+}

@@ -1,0 +1,191 @@
+"""Generate tests/golden/*.npz from the reference's OWN serial Sparse BLAS.
+
+Run in a checkout where the reference sources are present (they are compiled
+into oracle/_ref/libasc_ref.so by oracle/build_oracle.py).  The fixtures pin:
+
+* ``known_answers.npz`` - the known-answer cases of the reference's tests,
+  re-run through the reference itself:
+    - tests/sparse/blas_test.cc:165-219 (compat SpMV, strided output with
+      untouched holes; alpha=2, beta=-0.5 and alpha=1, beta=0),
+    - tests/sparse/blas_test.cc:221-242 (row {1e20, 1, -1e20} sums to 0.0f in
+      stored order),
+    - tests/sparse/blas_test.cc:244-296 (zero columns: y = beta*y),
+    - tests/sparse_cuda/sparse_cuda_test.cc:239-352 (4x5 strided SpMV,
+      expected {-9,-26,7,-24} and, with beta = 0, {-2,-8,11,-2}),
+    - tests/sparse_cuda/sparse_cuda_test.cc:354-433 (2x2 unit stride, {15,29}),
+    - tests/sparse/standard_blas_test.cc:177-345 (standard SpMV/SpMM on the
+      real part of the 2x2 matrix, CSR none / transpose, CSC, row- and
+      column-major B).
+* ``random_cases.npz`` - seeded random CSR/CSC matrices, vectors and dense
+  right-hand sides with the reference's outputs for compat SpMV, standard SpMV
+  (none, transpose) and standard SpMM, FP32 and FP64, unit and non-unit
+  strides, empty rows.
+* ``laplacian.npz`` - the 5-point Laplacian on a 316 x 316 grid
+  (alpha = 1, beta = 0.5, x and y uniform[-1, 1] from seed 0): SHA-256 of the
+  reference's output bytes and a strided sample of the output.
+
+Usage:  python tests/golden/make_golden.py
+"""
+
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from asc_cpp_b200 import synthetic  # noqa: E402
+from oracle import (CSC, CSR, COL_MAJOR, OP_NONE, OP_TRANSPOSE,  # noqa: E402
+                    ROW_MAJOR, Reference, build_oracle)
+
+
+def _check(code: int) -> None:
+    if code != 0:
+        raise RuntimeError(f"reference returned ErrorCode {code}")
+
+
+def known_answers(ref: Reference) -> dict[str, np.ndarray]:
+    out: dict[str, np.ndarray] = {}
+    # blas_test.cc:123-125 matrix, 3x4
+    ptr = np.array([0, 2, 4, 5], np.int64)
+    idx = np.array([1, 3, 0, 2, 1], np.int64)
+    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+        val = np.array([2, -1, 4, 5, 3], dt)
+        x = np.array([2, -1, 3, 4], dt)
+        y = np.array([7, -90, 11, -91, 13, -92], dt)
+        _check(ref.compat_spmv(3, 4, ptr, idx, val, 2.0, x, -0.5, y, 1, 2))
+        out[f"blas_compat_a2_bm05_{tag}"] = y.copy()
+        y2 = np.array([np.nan, -90, np.nan, -91, np.nan, -92], dt)
+        _check(ref.compat_spmv(3, 4, ptr, idx, val, 1.0, x, 0.0, y2, 1, 2))
+        out[f"blas_compat_a1_b0_{tag}"] = y2.copy()
+        # zero columns: 3 rows, 0 columns, alpha 7, beta 2
+        yz = np.array([2, -3, 4], dt)
+        _check(ref.compat_spmv(3, 0, np.zeros(4, np.int64), np.zeros(0, np.int64),
+                               np.zeros(0, dt), 7.0, np.zeros(0, dt), 2.0, yz, 1, 1))
+        out[f"blas_zero_columns_{tag}"] = yz.copy()
+        # empty 3x4 with NaN output, beta = 0
+        ye = np.full(3, np.nan, dt)
+        _check(ref.compat_spmv(3, 4, np.zeros(4, np.int64), np.zeros(0, np.int64),
+                               np.zeros(0, dt), 1.0, np.zeros(4, dt), 0.0, ye, 1, 1))
+        out[f"blas_empty_{tag}"] = ye.copy()
+    # blas_test.cc:221-242 order test (float)
+    yo = np.array([-1.0], np.float32)
+    _check(ref.compat_spmv(1, 3, np.array([0, 3], np.int64), np.array([0, 1, 2], np.int64),
+                           np.array([1e20, 1, -1e20], np.float32), 1.0,
+                           np.ones(3, np.float32), 0.0, yo, 1, 1))
+    out["blas_order_f32"] = yo.copy()
+    # sparse_cuda_test.cc:239-352 (4x5, x stride 2, y stride 3)
+    ptr = np.array([0, 2, 3, 6, 8], np.int64)
+    idx = np.array([0, 3, 1, 0, 2, 4, 1, 4], np.int64)
+    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+        val = np.array([2, -1, 4, 7, 3, 5, -2, 6], dt)
+        pad = 91
+        x = np.array([1, pad, -2, pad, 3, pad, 4, pad, -1], dt)
+        y = np.array([10, pad, pad, 20, pad, pad, 30, pad, pad, 40], dt)
+        _check(ref.compat_spmv(4, 5, ptr, idx, val, 2.0, x, -0.5, y, 2, 3))
+        out[f"cuda_strided_{tag}"] = y.copy()
+        yn = np.full(10, np.nan, dt)
+        _check(ref.compat_spmv(4, 5, ptr, idx, val, 1.0, x, 0.0, yn, 2, 3))
+        out[f"cuda_strided_beta0_{tag}"] = yn.copy()
+        # sparse_cuda_test.cc:354-433
+        yu = np.array([1, 1], dt)
+        _check(ref.compat_spmv(2, 2, np.array([0, 1, 2], np.int64), np.array([0, 1], np.int64),
+                               np.array([2, 3], dt), 2.0, np.array([4, 5], dt), -1.0, yu, 1, 1))
+        out[f"cuda_unit_{tag}"] = yu.copy()
+    # standard_blas_test.cc:177-345 (real parts of its 2x2 matrix)
+    ptr = np.array([0, 1, 3], np.int64)
+    idx = np.array([0, 0, 1], np.int64)
+    cptr = np.array([0, 2, 3], np.int64)
+    cidx = np.array([0, 1, 1], np.int64)
+    for dt, tag in ((np.float64, "f64"), (np.float32, "f32")):
+        val = np.array([2.0, 1.0, 3.0], dt)
+        x = np.array([1.0, -1.0], dt)
+        for op, name in ((OP_NONE, "none"), (OP_TRANSPOSE, "transpose")):
+            y = np.zeros(2, dt)
+            _check(ref.standard_spmv(CSR, op, 2, 2, ptr, idx, val, 1.0, x, y))
+            out[f"std_spmv_csr_{name}_{tag}"] = y.copy()
+            y = np.zeros(2, dt)
+            _check(ref.standard_spmv(CSC, op, 2, 2, cptr, cidx, val, 1.0, x, y))
+            out[f"std_spmv_csc_{name}_{tag}"] = y.copy()
+        b = np.array([1.0, 2.0, 3.0, 4.0], dt)
+        c = np.zeros(4, dt)
+        _check(ref.standard_spmm(CSR, OP_NONE, 2, 2, ptr, idx, val, 1.0, b, 2, 2, ROW_MAJOR, 2,
+                                 c, 2, 2, ROW_MAJOR, 2))
+        out[f"std_spmm_row_{tag}"] = c.copy()
+        b = np.array([1.0, 3.0, 2.0, 4.0], dt)
+        c = np.zeros(4, dt)
+        _check(ref.standard_spmm(CSC, OP_TRANSPOSE, 2, 2, cptr, cidx, val, 1.0, b, 2, 2,
+                                 COL_MAJOR, 2, c, 2, 2, COL_MAJOR, 2))
+        out[f"std_spmm_csc_col_t_{tag}"] = c.copy()
+    return out
+
+
+def random_cases(ref: Reference) -> dict[str, np.ndarray]:
+    rng = np.random.default_rng(20240611)
+    out: dict[str, np.ndarray] = {}
+    case = 0
+    for dt in (np.float64, np.float32):
+        for rows, cols, max_len, empty in ((1, 1, 1, 0.0), (7, 5, 5, 0.3),
+                                           (64, 48, 20, 0.1), (200, 300, 40, 0.2),
+                                           (513, 129, 70, 0.05)):
+            a = synthetic.random_csr(rng, rows, cols, max_len, dt, empty)
+            x = rng.uniform(-1, 1, cols).astype(dt)
+            xt = rng.uniform(-1, 1, rows).astype(dt)
+            y0 = rng.uniform(-1, 1, rows).astype(dt)
+            yt0 = rng.uniform(-1, 1, cols).astype(dt)
+            alpha, beta = float(rng.choice([1.0, -0.75, 2.5])), float(rng.choice([0.0, 0.5, -1.25]))
+            p = f"c{case}_"
+            out[p + "shape"] = np.array([rows, cols], np.int64)
+            out[p + "ptr"], out[p + "idx"], out[p + "val"] = a.ptr, a.idx, a.val
+            out[p + "x"], out[p + "xt"], out[p + "y0"], out[p + "yt0"] = x, xt, y0, yt0
+            out[p + "ab"] = np.array([alpha, beta])
+            y = y0.copy()
+            _check(ref.compat_spmv(rows, cols, a.ptr, a.idx, a.val, alpha, x, beta, y))
+            out[p + "compat"] = y
+            y = y0.copy()
+            _check(ref.standard_spmv(CSR, OP_NONE, rows, cols, a.ptr, a.idx, a.val, alpha, x, y))
+            out[p + "std_none"] = y
+            y = yt0.copy()
+            _check(ref.standard_spmv(CSR, OP_TRANSPOSE, rows, cols, a.ptr, a.idx, a.val, alpha,
+                                     xt, y))
+            out[p + "std_t"] = y
+            k = int(rng.choice([1, 3, 8, 33]))
+            b = rng.uniform(-1, 1, cols * k).astype(dt)
+            c = rng.uniform(-1, 1, rows * k).astype(dt)
+            out[p + "b"], out[p + "c0"] = b, c.copy()
+            _check(ref.standard_spmm(CSR, OP_NONE, rows, cols, a.ptr, a.idx, a.val, alpha, b,
+                                     cols, k, ROW_MAJOR, k, c, rows, k, ROW_MAJOR, k))
+            out[p + "spmm"] = c
+            case += 1
+    out["count"] = np.array([case])
+    return out
+
+
+def laplacian(ref: Reference) -> dict[str, np.ndarray]:
+    a = synthetic.laplacian_2d(316)
+    rng = np.random.default_rng(0)
+    x = rng.uniform(-1, 1, a.cols)
+    y = rng.uniform(-1, 1, a.rows)
+    _check(ref.compat_spmv(a.rows, a.cols, a.ptr, a.idx, a.val, 1.0, x, 0.5, y))
+    return {"sha256": np.frombuffer(hashlib.sha256(y.tobytes()).digest(), np.uint8),
+            "sample_index": np.arange(0, a.rows, 997, dtype=np.int64),
+            "sample": y[::997].copy()}
+
+
+def main() -> None:
+    build_oracle.build_reference()
+    ref = Reference()
+    np.savez_compressed(os.path.join(HERE, "known_answers.npz"), **known_answers(ref))
+    np.savez_compressed(os.path.join(HERE, "random_cases.npz"), **random_cases(ref))
+    np.savez_compressed(os.path.join(HERE, "laplacian.npz"), **laplacian(ref))
+    for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz"):
+        print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

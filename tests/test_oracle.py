@@ -1,0 +1,175 @@
+"""Pins the C restatement (oracle/sparse_oracle.c) before anything trusts it:
+against the reference's known answers (tests/golden/known_answers.npz), the
+reference's outputs on seeded random cases (tests/golden/random_cases.npz) and,
+where the reference harness is built, bit-exactly against it directly."""
+
+import numpy as np
+import pytest
+
+from oracle import CSC, CSR, COL_MAJOR, OP_NONE, OP_TRANSPOSE, ROW_MAJOR
+
+
+def _bits_equal(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return a.dtype == b.dtype and a.shape == b.shape and a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_known_answers_compat(restatement, known_answers, tag, dt):
+    ptr = np.array([0, 2, 4, 5], np.int64)
+    idx = np.array([1, 3, 0, 2, 1], np.int64)
+    val = np.array([2, -1, 4, 5, 3], dt)
+    x = np.array([2, -1, 3, 4], dt)
+    y = np.array([7, -90, 11, -91, 13, -92], dt)
+    restatement.compat_spmv(ptr, idx, val, 2.0, x, -0.5, y, 1, 2)
+    assert _bits_equal(y, known_answers[f"blas_compat_a2_bm05_{tag}"])
+    np.testing.assert_array_equal(y[::2], np.array([-15.5, 40.5, -12.5], dt))
+    y2 = np.array([np.nan, -90, np.nan, -91, np.nan, -92], dt)
+    restatement.compat_spmv(ptr, idx, val, 1.0, x, 0.0, y2, 1, 2)
+    assert _bits_equal(y2, known_answers[f"blas_compat_a1_b0_{tag}"])
+    # zero columns: y = beta * y
+    yz = np.array([2, -3, 4], dt)
+    restatement.compat_spmv(np.zeros(4, np.int64), np.zeros(0, np.int64), np.zeros(0, dt),
+                            7.0, np.zeros(0, dt), 2.0, yz)
+    assert _bits_equal(yz, known_answers[f"blas_zero_columns_{tag}"])
+
+
+def test_known_answer_order(restatement, known_answers):
+    y = np.array([-1.0], np.float32)
+    restatement.compat_spmv(np.array([0, 3], np.int64), np.array([0, 1, 2], np.int64),
+                            np.array([1e20, 1, -1e20], np.float32), 1.0,
+                            np.ones(3, np.float32), 0.0, y)
+    assert y[0] == 0.0 and _bits_equal(y, known_answers["blas_order_f32"])
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_known_answers_cuda_cases(restatement, known_answers, tag, dt):
+    ptr = np.array([0, 2, 3, 6, 8], np.int64)
+    idx = np.array([0, 3, 1, 0, 2, 4, 1, 4], np.int64)
+    val = np.array([2, -1, 4, 7, 3, 5, -2, 6], dt)
+    x = np.array([1, 91, -2, 91, 3, 91, 4, 91, -1], dt)
+    y = np.array([10, 91, 91, 20, 91, 91, 30, 91, 91, 40], dt)
+    restatement.compat_spmv(ptr, idx, val, 2.0, x, -0.5, y, 2, 3)
+    assert _bits_equal(y, known_answers[f"cuda_strided_{tag}"])
+    np.testing.assert_array_equal(y[::3], np.array([-9, -26, 7, -24], dt))
+    yu = np.array([1, 1], dt)
+    restatement.compat_spmv(np.array([0, 1, 2], np.int64), np.array([0, 1], np.int64),
+                            np.array([2, 3], dt), 2.0, np.array([4, 5], dt), -1.0, yu)
+    assert list(yu) == [15, 29]
+
+
+@pytest.mark.parametrize("tag,dt", [("f64", np.float64), ("f32", np.float32)])
+def test_known_answers_standard(restatement, known_answers, tag, dt):
+    ptr = np.array([0, 1, 3], np.int64)
+    idx = np.array([0, 0, 1], np.int64)
+    cptr = np.array([0, 2, 3], np.int64)
+    cidx = np.array([0, 1, 1], np.int64)
+    val = np.array([2.0, 1.0, 3.0], dt)
+    x = np.array([1.0, -1.0], dt)
+    for op, name in ((OP_NONE, "none"), (OP_TRANSPOSE, "transpose")):
+        y = np.zeros(2, dt)
+        restatement.standard_spmv(CSR, op, 2, 2, ptr, idx, val, 1.0, x, y)
+        assert _bits_equal(y, known_answers[f"std_spmv_csr_{name}_{tag}"])
+        y = np.zeros(2, dt)
+        restatement.standard_spmv(CSC, op, 2, 2, cptr, cidx, val, 1.0, x, y)
+        assert _bits_equal(y, known_answers[f"std_spmv_csc_{name}_{tag}"])
+    c = np.zeros(4, dt)
+    restatement.standard_spmm(CSR, OP_NONE, 2, 2, ptr, idx, val, 1.0,
+                              np.array([1, 2, 3, 4], dt), ROW_MAJOR, 2, c, ROW_MAJOR, 2, 2)
+    assert _bits_equal(c, known_answers[f"std_spmm_row_{tag}"])
+    c = np.zeros(4, dt)
+    restatement.standard_spmm(CSC, OP_TRANSPOSE, 2, 2, cptr, cidx, val, 1.0,
+                              np.array([1, 3, 2, 4], dt), COL_MAJOR, 2, c, COL_MAJOR, 2, 2)
+    assert _bits_equal(c, known_answers[f"std_spmm_csc_col_t_{tag}"])
+
+
+def test_random_cases_match_reference_outputs(restatement, random_cases):
+    n = int(random_cases["count"][0])
+    for case in range(n):
+        p = f"c{case}_"
+        rows, cols = (int(v) for v in random_cases[p + "shape"])
+        ptr, idx, val = random_cases[p + "ptr"], random_cases[p + "idx"], random_cases[p + "val"]
+        alpha, beta = (float(v) for v in random_cases[p + "ab"])
+        y = random_cases[p + "y0"].copy()
+        restatement.compat_spmv(ptr, idx, val, alpha, random_cases[p + "x"], beta, y)
+        assert _bits_equal(y, random_cases[p + "compat"]), case
+        y = random_cases[p + "y0"].copy()
+        restatement.standard_spmv(CSR, OP_NONE, rows, cols, ptr, idx, val, alpha,
+                                  random_cases[p + "x"], y)
+        assert _bits_equal(y, random_cases[p + "std_none"]), case
+        y = random_cases[p + "yt0"].copy()
+        restatement.standard_spmv(CSR, OP_TRANSPOSE, rows, cols, ptr, idx, val, alpha,
+                                  random_cases[p + "xt"], y)
+        assert _bits_equal(y, random_cases[p + "std_t"]), case
+        c = random_cases[p + "c0"].copy()
+        k = c.size // max(rows, 1)
+        restatement.standard_spmm(CSR, OP_NONE, rows, cols, ptr, idx, val, alpha,
+                                  random_cases[p + "b"], ROW_MAJOR, k, c, ROW_MAJOR, k, k)
+        assert _bits_equal(c, random_cases[p + "spmm"]), case
+
+
+def test_restatement_matches_reference_directly(restatement, reference):
+    """Fresh seeds each run: restatement and reference agree bit for bit,
+    including negative strides and CSC."""
+    from asc_cpp_b200 import synthetic
+    rng = np.random.default_rng()
+    for _ in range(20):
+        dt = rng.choice([np.float32, np.float64])
+        rows, cols = int(rng.integers(1, 120)), int(rng.integers(1, 120))
+        a = synthetic.random_csr(rng, rows, cols, int(rng.integers(1, 30)), dt, 0.2)
+        alpha, beta = float(rng.normal()), float(rng.choice([0.0, rng.normal()]))
+        x = rng.uniform(-1, 1, cols * 2).astype(dt)
+        y1 = rng.uniform(-1, 1, rows * 3).astype(dt)
+        y2 = y1.copy()
+        assert reference.compat_spmv(rows, cols, a.ptr, a.idx, a.val, alpha, x, beta, y1, 2, 3) == 0
+        restatement.compat_spmv(a.ptr, a.idx, a.val, alpha, x, beta, y2, 2, 3)
+        assert _bits_equal(y1, y2)
+        # standard, transpose, negative increments on both vectors
+        xt = rng.uniform(-1, 1, rows * 2).astype(dt)
+        yt1 = rng.uniform(-1, 1, cols).astype(dt)
+        yt2 = yt1.copy()
+        assert reference.standard_spmv(CSR, OP_TRANSPOSE, rows, cols, a.ptr, a.idx, a.val,
+                                       alpha, xt, yt1, incx=-2, incy=-1,
+                                       x_offset=2 * (rows - 1), y_offset=cols - 1) == 0
+        restatement.standard_spmv(CSR, OP_TRANSPOSE, rows, cols, a.ptr, a.idx, a.val, alpha,
+                                  xt, yt2, incx=-2, incy=-1, x_offset=2 * (rows - 1),
+                                  y_offset=cols - 1)
+        assert _bits_equal(yt1, yt2)
+        # CSC view of the same arrays (a is then cols x rows)
+        xc = rng.uniform(-1, 1, rows).astype(dt)
+        yc1 = rng.uniform(-1, 1, cols).astype(dt)
+        yc2 = yc1.copy()
+        assert reference.standard_spmv(CSC, OP_NONE, cols, rows, a.ptr, a.idx, a.val, alpha,
+                                       xc, yc1) == 0
+        restatement.standard_spmv(CSC, OP_NONE, cols, rows, a.ptr, a.idx, a.val, alpha, xc, yc2)
+        assert _bits_equal(yc1, yc2)
+
+
+def test_transpose_structure_is_stable_csc(restatement):
+    from asc_cpp_b200 import synthetic
+    rng = np.random.default_rng(5)
+    a = synthetic.random_csr(rng, 300, 200, 25, np.float64, 0.1)
+    t_ptr, t_idx, perm = restatement.transpose_structure(a.rows, a.cols, a.ptr, a.idx)
+    rows_of = np.repeat(np.arange(a.rows), np.diff(a.ptr))
+    order = np.lexsort((rows_of, a.idx))  # by column, then row
+    np.testing.assert_array_equal(perm, order)
+    np.testing.assert_array_equal(t_idx, rows_of[order])
+    np.testing.assert_array_equal(np.diff(t_ptr), np.bincount(a.idx, minlength=a.cols))
+
+
+def test_merge_path_split_properties(restatement):
+    from asc_cpp_b200 import synthetic
+    rng = np.random.default_rng(6)
+    a = synthetic.random_csr(rng, 500, 100, 30, np.float64, 0.3)
+    total = a.rows + a.nnz
+    prev = (0, 0)
+    for d in range(0, total + 1, 7):
+        r, z = restatement.merge_path_split(a.ptr, d)
+        assert r + z == d and r >= prev[0] and z >= prev[1]
+        # every row before r has ended by nonzero z; row r has not ended before z
+        if r > 0:
+            assert a.ptr[r] <= z
+        if r < a.rows:
+            assert a.ptr[r + 1] >= z
+        prev = (r, z)
