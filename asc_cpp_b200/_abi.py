@@ -74,8 +74,9 @@ class Variant(IntEnum):
     kAuto = -1
     kRowOrdered = 0
     kVector = 1
-    kMergePath = 2
-    kRowSplit = 3
+    kWarpTiles = 2
+    kMergePath = 3
+    kRowSplit = 4
 
 
 PLAN_TRANSPOSE = 1
@@ -157,7 +158,7 @@ def load(path: str | None = None) -> ctypes.CDLL:
     global _lib
     if _lib is not None and path is None:
         return _lib
-    path = path or LIB_PATH
+    path = path or os.environ.get("ASC_SB_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         raise ImportError(
             f"{path} is missing: build it with `python asc_cpp_b200/build.py` "
@@ -167,6 +168,5 @@ def load(path: str | None = None) -> ctypes.CDLL:
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if path == LIB_PATH:
-        _lib = lib
+    _lib = lib
     return lib

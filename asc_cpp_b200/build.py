@@ -60,7 +60,24 @@ def _compile(src: str, newest_header: float, verbose: bool) -> str:
     return obj
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, out: str | None = None,
+          defines: list[str] | None = None) -> str:
+    """Build the library (default: in-tree).  ``out``/``defines`` build an
+    experimental copy elsewhere with extra -D flags (own object directory)."""
+    global BUILD, COMMON
+    if out is not None:
+        saved = (BUILD, COMMON)
+        BUILD = os.path.join(os.path.dirname(os.path.abspath(out)), "_objs_" +
+                             os.path.basename(out).replace(".", "_"))
+        COMMON = COMMON + ["-D" + d for d in (defines or [])]
+        try:
+            return _build(force, verbose, out)
+        finally:
+            BUILD, COMMON = saved
+    return _build(force, verbose, LIB)
+
+
+def _build(force: bool, verbose: bool, lib: str) -> str:
     os.makedirs(BUILD, exist_ok=True)
     srcs = sources()
     newest_header = max((os.path.getmtime(h) for h in _headers()), default=0.0)
@@ -71,13 +88,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
                 os.remove(o)
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
         objs = list(ex.map(lambda s: _compile(s, newest_header, verbose), srcs))
-    if (force or not os.path.exists(LIB) or
-            any(os.path.getmtime(o) > os.path.getmtime(LIB) for o in objs)):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs
+    if (force or not os.path.exists(lib) or
+            any(os.path.getmtime(o) > os.path.getmtime(lib) for o in objs)):
+        cmd = [NVCC] + ARCH + ["-shared", "-o", lib] + objs
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"nvcc link failed:\n{res.stdout}\n{res.stderr}")
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

@@ -42,4 +42,22 @@ __device__ __forceinline__ T shfl_xor(T v, int mask, int width = 32) {
   return __shfl_xor_sync(0xffffffffu, v, mask, width);
 }
 
+// First row r in [0, rows] with weight*r + ptr[r] >= target.  The key is
+// strictly increasing in r, so row tiles defined by it are contiguous, and a
+// tile spanning `items` keys holds at most items/weight rows.
+__device__ __forceinline__ int64_t first_row_at(const int64_t* __restrict__ ptr, int64_t rows,
+                                                int64_t weight, int64_t target) {
+  int64_t lo = 0;
+  int64_t hi = rows;
+  while (lo < hi) {
+    const int64_t mid = lo + ((hi - lo) >> 1);
+    if (weight * mid + __ldg(ptr + mid) < target) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
 }  // namespace ascb

@@ -122,14 +122,18 @@ Status ValidateContext(asc_sb_context* ctx) {
   return Status::Ok();
 }
 
+// Number of warp row tiles of a CSR structure.
+std::int64_t WarpTiles(std::int64_t rows, std::int64_t nnz) {
+  return ascb_row_tile_count(rows, nnz, ascb_warp_tile_items(), ascb_warp_tile_row_weight());
+}
+
 // ---- workspace layout of asc_sb_csr_spmv ----------------------------------
 // The size is a function of the matrix shape only, so it is stable for a given
-// (A, x, y) (the reference's rule, operations.cc:884-909): room for the
-// row-ordered tile bounds.
+// (A, x, y) (the reference's rule, operations.cc:884-909): room for the warp
+// row-tile bounds.
 std::size_t CompatWorkspaceBytes(const asc_sb_sparse& m) {
   if (m.rows == 0 || m.columns == 0) return 0;
-  const std::int64_t tiles = ascb_row_tile_count(
-      m.rows, m.nonzeros, ascb_row_ordered_items(Dtype(m.element_kind)));
+  const std::int64_t tiles = WarpTiles(m.rows, m.nonzeros);
   return RoundUp(static_cast<std::size_t>(tiles + 1) * sizeof(std::int64_t), 256);
 }
 
@@ -164,27 +168,30 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
               const ascb_csr& a, int dtype, double alpha, double beta,
               const ascb_vec& x, const ascb_vec& y, std::int64_t* tile_buffer,
               const std::int64_t* planned_tiles) {
-  if (choice.variant == ASC_SB_VARIANT_VECTOR || choice.variant == ASC_SB_VARIANT_MERGE_PATH ||
-      choice.variant == ASC_SB_VARIANT_ROW_SPLIT) {
+  if (choice.variant == ASC_SB_VARIANT_VECTOR) {
     const int lanes = choice.lanes > 0 ? choice.lanes : 4;
     return Launched(ctx,
                     ascb_spmv_vector(ctx->stream, dtype, form, lanes, &a, alpha, beta, &x, &y,
                                      ctx->sm_count),
                     "CUDA could not launch the vector CSR SpMV kernel");
   }
-  const std::int64_t items = ascb_row_ordered_items(dtype);
-  const std::int64_t tiles = ascb_row_tile_count(a.rows, a.nnz, items);
+  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) share the warp-tiled
+  // kernel and its partition.
+  const int exact = choice.variant == ASC_SB_VARIANT_ROW_ORDERED ? 1 : 0;
+  const std::int64_t tiles = WarpTiles(a.rows, a.nnz);
   const std::int64_t* tiles_ptr = planned_tiles;
   if (tiles_ptr == nullptr && tile_buffer != nullptr) {
-    Status s = Launched(ctx, ascb_row_tiles(ctx->stream, &a, items, tile_buffer, tiles),
+    Status s = Launched(ctx,
+                        ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
+                                       ascb_warp_tile_row_weight(), tile_buffer, tiles),
                         "CUDA could not launch the row-tile partition kernel");
     if (!s.ok()) return s;
     tiles_ptr = tile_buffer;
   }
   return Launched(ctx,
-                  ascb_spmv_row_ordered(ctx->stream, dtype, form, &a, alpha, beta, &x, &y,
-                                        tiles_ptr, tiles),
-                  "CUDA could not launch the row-ordered SpMV kernel");
+                  ascb_spmv_warp(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
+                                 tiles_ptr, tiles, ctx->sm_count),
+                  "CUDA could not launch the warp-tiled SpMV kernel");
 }
 
 struct CompatOperands {
@@ -285,6 +292,9 @@ int asc_sb_context_set_variant(asc_sb_context* ctx, int32_t variant, int32_t lan
   const bool lanes_ok = lanes == 0 || (lanes > 0 && lanes <= 32 && (lanes & (lanes - 1)) == 0);
   if (variant < ASC_SB_VARIANT_AUTO || variant > ASC_SB_VARIANT_ROW_SPLIT || !lanes_ok) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Unknown SpMV variant or lane count"));
+  }
+  if (variant == ASC_SB_VARIANT_MERGE_PATH || variant == ASC_SB_VARIANT_ROW_SPLIT) {
+    return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "This SpMV variant is not available yet"));
   }
   std::lock_guard<std::mutex> lock(ctx->mutex);
   ctx->variant = variant;
@@ -545,8 +555,7 @@ int asc_sb_plan_workspace_size(asc_sb_context* ctx, const asc_sb_sparse* m, int3
     return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "transposed plans are not built yet"));
   }
   const std::int64_t outer = m->format == ASC_SB_CSC ? m->columns : m->rows;
-  const std::int64_t tiles =
-      ascb_row_tile_count(outer, m->nonzeros, ascb_row_ordered_items(Dtype(m->element_kind)));
+  const std::int64_t tiles = WarpTiles(outer, m->nonzeros);
   *bytes = RoundUp(static_cast<std::size_t>(tiles + 1) * 8, 256);
   return Finish(ctx, Status::Ok());
 }
@@ -579,11 +588,12 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
   plan->flags = flags;
   const bool csc = m->format == ASC_SB_CSC;
   const ascb_csr a = AsCsr(*m, csc);
-  const std::int64_t items = ascb_row_ordered_items(Dtype(m->element_kind));
-  plan->row_tiles = ascb_row_tile_count(a.rows, a.nnz, items);
+  plan->row_tiles = WarpTiles(a.rows, a.nnz);
   plan->tile_row = static_cast<std::int64_t*>(workspace);
   if (plan->row_tiles > 0) {
-    s = Launched(ctx, ascb_row_tiles(ctx->stream, &a, items, plan->tile_row, plan->row_tiles),
+    s = Launched(ctx,
+                 ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
+                                ascb_warp_tile_row_weight(), plan->tile_row, plan->row_tiles),
                  "CUDA could not launch the row-tile partition kernel");
     if (!s.ok()) {
       delete plan;

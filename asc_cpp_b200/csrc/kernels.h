@@ -33,10 +33,10 @@ enum { ASCB_COL_MAJOR = 0, ASCB_ROW_MAJOR = 1 };
 enum { ASCB_COMPAT = 0, ASCB_STANDARD = 1 };
 
 // ---- partitions (integer work, bit-exact) ----
-// Row tiles of the row-ordered kernel: tile k owns rows r with
-// r + ptr[r] in [k*items, (k+1)*items).  Writes ntiles+1 row bounds.
-int64_t ascb_row_tile_count(int64_t rows, int64_t nnz, int64_t items);
-int ascb_row_tiles(void* stream, const ascb_csr* a, int64_t items,
+// Row tiles: tile k owns rows r with weight*r + ptr[r] in
+// [k*items, (k+1)*items).  Writes ntiles+1 row bounds.
+int64_t ascb_row_tile_count(int64_t rows, int64_t nnz, int64_t items, int64_t weight);
+int ascb_row_tiles(void* stream, const ascb_csr* a, int64_t items, int64_t weight,
                    int64_t* tile_row, int64_t ntiles);
 // Merge-path split points of diagonals k*items, k = 0..ntiles (row, nnz).
 int64_t ascb_merge_tile_count(int64_t rows, int64_t nnz, int64_t items);
@@ -45,12 +45,14 @@ int ascb_merge_path_splits(void* stream, const ascb_csr* a, int64_t items,
                            int64_t ntiles);
 
 // ---- SpMV variants ----
-// Bit-exact row-ordered SpMV (tiles from ascb_row_tiles with the same items).
-int64_t ascb_row_ordered_items(int dtype);
-int ascb_spmv_row_ordered(void* stream, int dtype, int form, const ascb_csr* a,
-                          double alpha, double beta, const ascb_vec* x,
-                          const ascb_vec* y, const int64_t* tile_row,
-                          int64_t ntiles);
+// Warp-tiled SpMV over row tiles of ascb_warp_tile_items() weighted items with
+// row weight ascb_warp_tile_row_weight().  exact = 1 reproduces the serial
+// reference bit for bit.  tile_row may be NULL (bounds searched in-kernel).
+int64_t ascb_warp_tile_items(void);
+int64_t ascb_warp_tile_row_weight(void);
+int ascb_spmv_warp(void* stream, int dtype, int form, int exact, const ascb_csr* a,
+                   double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
+                   const int64_t* tile_row, int64_t ntiles, int sm_count);
 // Vector CSR: `lanes` (1..32, power of two) threads per row.
 int ascb_spmv_vector(void* stream, int dtype, int form, int lanes,
                      const ascb_csr* a, double alpha, double beta,

@@ -8,26 +8,14 @@ namespace {
 
 constexpr int kPartitionThreads = 256;
 
-// Tile k starts at the first row r with r + ptr[r] >= k * items.
-// f(r) = r + ptr[r] is strictly increasing, so the search is well defined;
-// f(rows) = rows + nnz bounds every target.
+// Tile k starts at the first row r with weight*r + ptr[r] >= k*items; the
+// last bound is `rows`.
 __global__ void __launch_bounds__(kPartitionThreads)
-row_tile_kernel(int64_t rows, const int64_t* __restrict__ ptr, int64_t items,
+row_tile_kernel(int64_t rows, const int64_t* __restrict__ ptr, int64_t items, int64_t weight,
                 int64_t* __restrict__ tile_row, int64_t ntiles) {
   const int64_t k = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
   if (k > ntiles) return;
-  const int64_t target = k * items;
-  int64_t lo = 0;
-  int64_t hi = rows;
-  while (lo < hi) {
-    const int64_t mid = lo + ((hi - lo) >> 1);
-    if (mid + __ldg(ptr + mid) < target) {
-      lo = mid + 1;
-    } else {
-      hi = mid;
-    }
-  }
-  tile_row[k] = k == ntiles ? rows : lo;
+  tile_row[k] = k == ntiles ? rows : first_row_at(ptr, rows, weight, k * items);
 }
 
 // Merge-path split of diagonal d: the first i in [max(0, d-nnz), min(d, rows)]
@@ -54,25 +42,26 @@ merge_split_kernel(int64_t rows, const int64_t* __restrict__ ptr, int64_t nnz,
   split_nz[k] = d - lo;
 }
 
+unsigned blocks_for(int64_t threads) {
+  return static_cast<unsigned>((threads + kPartitionThreads - 1) / kPartitionThreads);
+}
+
 }  // namespace
 }  // namespace ascb
 
 extern "C" {
 
-int64_t ascb_row_tile_count(int64_t rows, int64_t nnz, int64_t items) {
+int64_t ascb_row_tile_count(int64_t rows, int64_t nnz, int64_t items, int64_t weight) {
   if (rows <= 0) return 0;
-  return (rows + nnz + items - 1) / items;
+  return (weight * rows + nnz + items - 1) / items;
 }
 
-int ascb_row_tiles(void* stream, const ascb_csr* a, int64_t items,
+int ascb_row_tiles(void* stream, const ascb_csr* a, int64_t items, int64_t weight,
                    int64_t* tile_row, int64_t ntiles) {
   if (ntiles <= 0) return 0;
-  const int64_t threads = ntiles + 1;
-  const unsigned blocks = static_cast<unsigned>(
-      (threads + ascb::kPartitionThreads - 1) / ascb::kPartitionThreads);
-  ascb::row_tile_kernel<<<blocks, ascb::kPartitionThreads, 0,
-                          static_cast<cudaStream_t>(stream)>>>(
-      a->rows, a->ptr, items, tile_row, ntiles);
+  ascb::row_tile_kernel<<<ascb::blocks_for(ntiles + 1), ascb::kPartitionThreads, 0,
+                          static_cast<cudaStream_t>(stream)>>>(a->rows, a->ptr, items, weight,
+                                                               tile_row, ntiles);
   return static_cast<int>(cudaGetLastError());
 }
 
@@ -82,13 +71,9 @@ int64_t ascb_merge_tile_count(int64_t rows, int64_t nnz, int64_t items) {
 }
 
 int ascb_merge_path_splits(void* stream, const ascb_csr* a, int64_t items,
-                           int64_t* split_row, int64_t* split_nz,
-                           int64_t ntiles) {
+                           int64_t* split_row, int64_t* split_nz, int64_t ntiles) {
   if (ntiles <= 0) return 0;
-  const int64_t threads = ntiles + 1;
-  const unsigned blocks = static_cast<unsigned>(
-      (threads + ascb::kPartitionThreads - 1) / ascb::kPartitionThreads);
-  ascb::merge_split_kernel<<<blocks, ascb::kPartitionThreads, 0,
+  ascb::merge_split_kernel<<<ascb::blocks_for(ntiles + 1), ascb::kPartitionThreads, 0,
                              static_cast<cudaStream_t>(stream)>>>(
       a->rows, a->ptr, a->nnz, items, split_row, split_nz, ntiles);
   return static_cast<int>(cudaGetLastError());

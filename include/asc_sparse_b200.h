@@ -87,11 +87,12 @@ enum { ASC_SB_DETERMINISTIC = 0, ASC_SB_BACKEND_DEFAULT = 1 };
 /* SpMV kernel variants (no reference counterpart; the reference has one
  * thread-per-row kernel, src/sparse/cuda/kernels.cu:91-115). */
 enum {
-  ASC_SB_VARIANT_AUTO = -1,      /* library choice (selector / heuristics) */
-  ASC_SB_VARIANT_ROW_ORDERED = 0,/* bit-exact serial order, CTA row tiles   */
-  ASC_SB_VARIANT_VECTOR = 1,     /* 'lanes' threads per row, shuffle sums   */
-  ASC_SB_VARIANT_MERGE_PATH = 2, /* merge-path balanced tiles + fix-up      */
-  ASC_SB_VARIANT_ROW_SPLIT = 3   /* vector rows + long rows split over CTAs */
+  ASC_SB_VARIANT_AUTO = -1,       /* library choice (selector / heuristics)   */
+  ASC_SB_VARIANT_ROW_ORDERED = 0, /* warp row tiles, bit-exact serial order   */
+  ASC_SB_VARIANT_VECTOR = 1,      /* 'lanes' threads per row, shuffle sums    */
+  ASC_SB_VARIANT_WARP_TILES = 2,  /* warp row tiles, FMA, parallel long rows  */
+  ASC_SB_VARIANT_MERGE_PATH = 3,  /* merge-path balanced tiles + carry fix-up */
+  ASC_SB_VARIANT_ROW_SPLIT = 4    /* vector rows + long rows split over CTAs  */
 };
 
 /* ---- descriptors ---------------------------------------------------------- */
