@@ -24,8 +24,22 @@ __device__ __forceinline__ int64_t ld_stream(const int64_t* p) {
 }
 
 // Gathered operand (x): read-only path, cached in L1 and L2.
+#ifndef ASCB_GATHER_NOALLOC
 template <typename T>
 __device__ __forceinline__ T ld_gather(const T* p) { return __ldg(p); }
+#else
+// variant: no L1 allocation for the gathers
+__device__ __forceinline__ double ld_gather(const double* p) {
+  double v;
+  asm volatile("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_gather(const float* p) {
+  float v;
+  asm volatile("ld.global.nc.L1::no_allocate.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+#endif
 
 // Strided element access; `stride` may be negative (pointer = logical 0).
 template <bool UNIT, typename T>

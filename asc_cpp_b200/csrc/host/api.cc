@@ -34,21 +34,27 @@ struct asc_sb_context {
   std::mutex mutex;
   std::string last_error;
   std::atomic<std::int64_t> launches{0};
+  int* status = nullptr;  // device word: kernels record bounded-wait timeouts
+};
+
+// Partitions of one CSR structure, as the kernels consume them.
+struct Partitions {
+  const std::int64_t* warp_tiles = nullptr;    // ascb_row_tiles, warp-tile weights
+  std::int64_t n_warp = 0;
+  const std::int64_t* merge_bounds = nullptr;  // ascb_merge_bounds pairs
+  std::int64_t n_merge = 0;
 };
 
 struct asc_sb_plan {
   asc_sb_sparse matrix{};
   int flags = 0;
-  // row-ordered tiles
-  std::int64_t* tile_row = nullptr;
-  std::int64_t row_tiles = 0;
-  // transposed structure (CSR of A^T) with its values
+  Partitions part;    // of the stored arrays read as CSR
+  // transposed structure (CSR of the transpose of the stored arrays)
   std::int64_t* t_ptr = nullptr;
   std::int64_t* t_idx = nullptr;
   void* t_val = nullptr;
   std::int64_t* t_perm = nullptr;
-  std::int64_t* t_tile_row = nullptr;
-  std::int64_t t_row_tiles = 0;
+  Partitions t_part;
 };
 
 namespace {
@@ -126,15 +132,20 @@ Status ValidateContext(asc_sb_context* ctx) {
 std::int64_t WarpTiles(std::int64_t rows, std::int64_t nnz) {
   return ascb_row_tile_count(rows, nnz, ascb_warp_tile_items(), ascb_warp_tile_row_weight());
 }
+std::size_t WarpTileBytes(std::int64_t rows, std::int64_t nnz) {
+  return RoundUp(static_cast<std::size_t>(WarpTiles(rows, nnz) + 1) * 8, 256);
+}
+std::size_t MergeBoundBytes(std::int64_t rows, std::int64_t nnz) {
+  return RoundUp(static_cast<std::size_t>(ascb_merge_tiles(rows, nnz) + 1) * 16, 256);
+}
 
 // ---- workspace layout of asc_sb_csr_spmv ----------------------------------
 // The size is a function of the matrix shape only, so it is stable for a given
-// (A, x, y) (the reference's rule, operations.cc:884-909): room for the warp
-// row-tile bounds.
+// (A, x, y) (the reference's rule, operations.cc:884-909): room for the
+// partition of whichever kernel the context selects.
 std::size_t CompatWorkspaceBytes(const asc_sb_sparse& m) {
   if (m.rows == 0 || m.columns == 0) return 0;
-  const std::int64_t tiles = WarpTiles(m.rows, m.nonzeros);
-  return RoundUp(static_cast<std::size_t>(tiles + 1) * sizeof(std::int64_t), 256);
+  return std::max(WarpTileBytes(m.rows, m.nonzeros), MergeBoundBytes(m.rows, m.nonzeros));
 }
 
 // Choice of SpMV kernel for a real CSR product.
@@ -159,15 +170,17 @@ Choice Choose(const asc_sb_context* ctx, const asc_sb_sparse& m) {
     c.lanes = ctx->lanes > 0 ? ctx->lanes : AutoLanes(m, false);
     return c;
   }
-  c.variant = ASC_SB_VARIANT_VECTOR;
-  c.lanes = AutoLanes(m, false);
+  c.variant = ASC_SB_VARIANT_WARP_TILES;
   return c;
 }
 
+// Runs one real CSR SpMV with the chosen kernel.  Partitions come from the
+// plan when there is one, else are built into `scratch` (caller workspace),
+// else the kernel that searches its own tile bounds is used.
 Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
               const ascb_csr& a, int dtype, double alpha, double beta,
-              const ascb_vec& x, const ascb_vec& y, std::int64_t* tile_buffer,
-              const std::int64_t* planned_tiles) {
+              const ascb_vec& x, const ascb_vec& y, std::int64_t* scratch,
+              const Partitions* planned) {
   if (choice.variant == ASC_SB_VARIANT_VECTOR) {
     const int lanes = choice.lanes > 0 ? choice.lanes : 4;
     return Launched(ctx,
@@ -175,23 +188,72 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
                                      ctx->sm_count),
                     "CUDA could not launch the vector CSR SpMV kernel");
   }
-  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) share the warp-tiled
-  // kernel and its partition.
   const int exact = choice.variant == ASC_SB_VARIANT_ROW_ORDERED ? 1 : 0;
+  if (choice.variant == ASC_SB_VARIANT_MERGE_PATH) {
+    const std::int64_t tiles = ascb_merge_tiles(a.rows, a.nnz);
+    const std::int64_t* bounds = planned != nullptr ? planned->merge_bounds : nullptr;
+    if (bounds == nullptr && scratch != nullptr) {
+      Status s = Launched(ctx, ascb_merge_bounds(ctx->stream, &a, scratch, tiles),
+                          "CUDA could not launch the merge partition kernel");
+      if (!s.ok()) return s;
+      bounds = scratch;
+    }
+    if (bounds != nullptr) {
+      return Launched(ctx,
+                      ascb_spmv_merge(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
+                                      bounds, tiles, ctx->sm_count, ctx->status),
+                      "CUDA could not launch the merge SpMV kernel");
+    }
+    // no partition buffer at all (zero-workspace calls): warp tiles with
+    // in-kernel bound search
+  }
   const std::int64_t tiles = WarpTiles(a.rows, a.nnz);
-  const std::int64_t* tiles_ptr = planned_tiles;
-  if (tiles_ptr == nullptr && tile_buffer != nullptr) {
+  const std::int64_t* tiles_ptr = planned != nullptr ? planned->warp_tiles : nullptr;
+  if (tiles_ptr == nullptr && scratch != nullptr) {
     Status s = Launched(ctx,
                         ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
-                                       ascb_warp_tile_row_weight(), tile_buffer, tiles),
+                                       ascb_warp_tile_row_weight(), scratch, tiles),
                         "CUDA could not launch the row-tile partition kernel");
     if (!s.ok()) return s;
-    tiles_ptr = tile_buffer;
+    tiles_ptr = scratch;
+  }
+  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) run the register-
+  // segmented kernel, which needs 16-byte aligned index and value arrays;
+  // otherwise the scalar-load warp kernel with the same numerics.
+  const bool aligned16 =
+      ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) & 15u) == 0;
+  if (aligned16) {
+    return Launched(ctx,
+                    ascb_spmv_seg(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
+                                  tiles_ptr, tiles, ctx->sm_count),
+                    "CUDA could not launch the segmented SpMV kernel");
   }
   return Launched(ctx,
                   ascb_spmv_warp(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
                                  tiles_ptr, tiles, ctx->sm_count),
                   "CUDA could not launch the warp-tiled SpMV kernel");
+}
+
+// Builds both partitions of `a` into `buffer` (plan memory).
+Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* buffer,
+                       Partitions* out) {
+  out->n_warp = WarpTiles(a.rows, a.nnz);
+  out->n_merge = ascb_merge_tiles(a.rows, a.nnz);
+  auto* warp = reinterpret_cast<std::int64_t*>(buffer);
+  auto* merge = reinterpret_cast<std::int64_t*>(buffer + WarpTileBytes(a.rows, a.nnz));
+  out->warp_tiles = warp;
+  out->merge_bounds = merge;
+  if (a.rows == 0) return Status::Ok();
+  Status s = Launched(ctx,
+                      ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
+                                     ascb_warp_tile_row_weight(), warp, out->n_warp),
+                      "CUDA could not launch the row-tile partition kernel");
+  if (!s.ok()) return s;
+  return Launched(ctx, ascb_merge_bounds(ctx->stream, &a, merge, out->n_merge),
+                  "CUDA could not launch the merge partition kernel");
+}
+std::size_t PartitionBytes(std::int64_t rows, std::int64_t nnz) {
+  return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz);
 }
 
 struct CompatOperands {
@@ -262,19 +324,46 @@ int asc_sb_context_create(int32_t device, void* stream, asc_sb_context** out) {
   } else {
     ctx->stream = static_cast<cudaStream_t>(stream);
   }
+  // One device word per context for kernels' bounded-wait timeouts (set-up
+  // allocation; no operation allocates).
+  if (cudaMalloc(reinterpret_cast<void**>(&ctx->status), sizeof(int)) != cudaSuccess ||
+      cudaMemset(ctx->status, 0, sizeof(int)) != cudaSuccess) {
+    (void)cudaGetLastError();
+    if (ctx->owns_stream) (void)cudaStreamDestroy(ctx->stream);
+    if (ctx->status != nullptr) (void)cudaFree(ctx->status);
+    delete ctx;
+    return ASC_SB_ALLOCATION;
+  }
   *out = ctx;
   return ASC_SB_OK;
 }
 
 int asc_sb_context_destroy(asc_sb_context* ctx) {
   if (ctx == nullptr) return ASC_SB_OK;
-  if (ctx->owns_stream) {
-    DeviceGuard guard(ctx->device);
-    (void)cudaStreamSynchronize(ctx->stream);
-    (void)cudaStreamDestroy(ctx->stream);
-  }
+  DeviceGuard guard(ctx->device);
+  (void)cudaStreamSynchronize(ctx->stream);
+  if (ctx->owns_stream) (void)cudaStreamDestroy(ctx->stream);
+  if (ctx->status != nullptr) (void)cudaFree(ctx->status);
   delete ctx;
   return ASC_SB_OK;
+}
+
+int asc_sb_context_device_status(asc_sb_context* ctx, int32_t* value, int32_t clear) {
+  if (ctx == nullptr) return ASC_SB_INVALID_STATE;
+  if (value == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "value cannot be null"));
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  int host = 0;
+  cudaError_t e = cudaMemcpyAsync(&host, ctx->status, sizeof(int), cudaMemcpyDeviceToHost,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess && clear) e = cudaMemsetAsync(ctx->status, 0, sizeof(int), ctx->stream);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return Finish(ctx, {ASC_SB_PROVIDER, std::string("status read failed: ") + cudaGetErrorString(e)});
+  }
+  *value = host;
+  return Finish(ctx, Status::Ok());
 }
 
 int asc_sb_context_set_determinism(asc_sb_context* ctx, int32_t determinism) {
@@ -293,7 +382,7 @@ int asc_sb_context_set_variant(asc_sb_context* ctx, int32_t variant, int32_t lan
   if (variant < ASC_SB_VARIANT_AUTO || variant > ASC_SB_VARIANT_ROW_SPLIT || !lanes_ok) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Unknown SpMV variant or lane count"));
   }
-  if (variant == ASC_SB_VARIANT_MERGE_PATH || variant == ASC_SB_VARIANT_ROW_SPLIT) {
+  if (variant == ASC_SB_VARIANT_ROW_SPLIT) {
     return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "This SpMV variant is not available yet"));
   }
   std::lock_guard<std::mutex> lock(ctx->mutex);
@@ -450,9 +539,8 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
   const ascb_vec xv = AsVec(x), yv = AsVec(y);
   if (!transposed) {
     const Choice choice = Choose(ctx, m);
-    const std::int64_t* planned =
-        (plan != nullptr && choice.variant == ASC_SB_VARIANT_ROW_ORDERED) ? plan->tile_row : nullptr;
-    return RunCsr(ctx, choice, ASCB_STANDARD, a, dtype, alpha, 0.0, xv, yv, nullptr, planned);
+    return RunCsr(ctx, choice, ASCB_STANDARD, a, dtype, alpha, 0.0, xv, yv, nullptr,
+                  plan != nullptr ? &plan->part : nullptr);
   }
   if (plan != nullptr && plan->t_ptr != nullptr) {
     ascb_csr t{};
@@ -462,9 +550,9 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
     t.ptr = plan->t_ptr;
     t.idx = plan->t_idx;
     t.val = plan->t_val;
-    Choice choice = Choose(ctx, m);
+    const Choice choice = Choose(ctx, m);
     return RunCsr(ctx, choice, ASCB_STANDARD, t, dtype, alpha, 0.0, xv, yv, nullptr,
-                  choice.variant == ASC_SB_VARIANT_ROW_ORDERED ? plan->t_tile_row : nullptr);
+                  &plan->t_part);
   }
   if (ctx->determinism == ASC_SB_DETERMINISTIC) {
     return Fail(ASC_SB_INVALID_STATE,
@@ -555,8 +643,7 @@ int asc_sb_plan_workspace_size(asc_sb_context* ctx, const asc_sb_sparse* m, int3
     return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "transposed plans are not built yet"));
   }
   const std::int64_t outer = m->format == ASC_SB_CSC ? m->columns : m->rows;
-  const std::int64_t tiles = WarpTiles(outer, m->nonzeros);
-  *bytes = RoundUp(static_cast<std::size_t>(tiles + 1) * 8, 256);
+  *bytes = PartitionBytes(outer, m->nonzeros);
   return Finish(ctx, Status::Ok());
 }
 
@@ -588,17 +675,10 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
   plan->flags = flags;
   const bool csc = m->format == ASC_SB_CSC;
   const ascb_csr a = AsCsr(*m, csc);
-  plan->row_tiles = WarpTiles(a.rows, a.nnz);
-  plan->tile_row = static_cast<std::int64_t*>(workspace);
-  if (plan->row_tiles > 0) {
-    s = Launched(ctx,
-                 ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
-                                ascb_warp_tile_row_weight(), plan->tile_row, plan->row_tiles),
-                 "CUDA could not launch the row-tile partition kernel");
-    if (!s.ok()) {
-      delete plan;
-      return Finish(ctx, s);
-    }
+  s = BuildPartitions(ctx, a, static_cast<unsigned char*>(workspace), &plan->part);
+  if (!s.ok()) {
+    delete plan;
+    return Finish(ctx, s);
   }
   *out = plan;
   return Finish(ctx, Status::Ok());
@@ -629,7 +709,7 @@ int asc_sb_plan_csr_spmv(asc_sb_context* ctx, const asc_sb_plan* plan, double al
   const ascb_csr a = AsCsr(plan->matrix, false);
   const Choice choice = Choose(ctx, plan->matrix);
   s = RunCsr(ctx, choice, ASCB_COMPAT, a, Dtype(plan->matrix.element_kind), alpha, beta,
-             AsVec(*x), AsVec(*y), nullptr, plan->tile_row);
+             AsVec(*x), AsVec(*y), nullptr, &plan->part);
   return Finish(ctx, s);
 }
 

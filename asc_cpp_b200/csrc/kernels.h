@@ -53,6 +53,19 @@ int64_t ascb_warp_tile_row_weight(void);
 int ascb_spmv_warp(void* stream, int dtype, int form, int exact, const ascb_csr* a,
                    double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
                    const int64_t* tile_row, int64_t ntiles, int sm_count);
+// Merge-based, TMA-fed SpMV.  bounds[2k], bounds[2k+1] = first row of tile
+// k and ptr[that row], k = 0..ntiles (ascb_merge_bounds).  exact = 1 is
+// bit-exact.  status (nullable) receives 1 if a bounded wait gave up.
+int64_t ascb_merge_tiles(int64_t rows, int64_t nnz);
+int ascb_merge_bounds(void* stream, const ascb_csr* a, int64_t* bounds, int64_t ntiles);
+int ascb_spmv_merge(void* stream, int dtype, int form, int exact, const ascb_csr* a,
+                    double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
+                    const int64_t* bounds, int64_t ntiles, int sm_count, int* status);
+// Register-segmented SpMV over the warp row tiles (exact = 1: bit-exact);
+// requires the column-index and value arrays to start on 16-byte boundaries.
+int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
+                  double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
+                  int64_t ntiles, int sm_count);
 // Vector CSR: `lanes` (1..32, power of two) threads per row.
 int ascb_spmv_vector(void* stream, int dtype, int form, int lanes,
                      const ascb_csr* a, double alpha, double beta,

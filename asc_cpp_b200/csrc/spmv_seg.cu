@@ -1,0 +1,438 @@
+// Register-segmented CSR SpMV for sm_100a (the default SpMV kernel, both
+// numerical modes).
+//
+// Tiles are the warp row tiles of the partition kernel (weight W = 8, 256
+// weighted items: at most 32 rows, all but the last shorter than 256
+// nonzeros).  For one tile:
+//   * the window of at most 256 nonzero positions is split into 32 lanes x 8
+//     CONTIGUOUS positions, so each lane fetches its column indices and values
+//     with 128-bit vector loads (every sector fully used) straight into
+//     registers and keeps 8 independent x gathers in flight;
+//   * a 256-bit shared bitmap marks the positions where rows start; each lane
+//     runs a segmented sum over its 8 products, closing a row at every start;
+//   * rows that cross lane boundaries are joined, and the lane that holds a
+//     row's last product writes y:
+//       FAST  -- one segmented warp scan of the lanes' open partial sums;
+//                |y - y_ref| <= gamma_{n+2}(|alpha||A||x| + |beta||y|);
+//       EXACT -- the running sum is handed lane to lane in stored order (a
+//                lane waits only if its first position continues a row), so
+//                every row is summed exactly as the serial reference does.
+// No shared-memory product buffer, no per-row loop: lane utilisation does not
+// depend on the row-length distribution.  The last row of a tile may be long;
+// its remainder past the window is reduced by the whole warp (EXACT: in
+// stored order by one lane).
+#include "common.cuh"
+#include "kernels.h"
+
+namespace ascb {
+namespace {
+
+constexpr int kWarpsPerCta = 4;
+constexpr int kThreads = kWarpsPerCta * 32;
+constexpr int kItems = 256;        // weighted items per tile (= positions)
+constexpr int kRowWeight = kItems / 32;
+constexpr int kPer = 8;            // contiguous positions per lane
+constexpr int kChunk = 32;         // tile bounds cached per warp
+constexpr int kMaxDevices = 64;
+#ifndef ASCB_SEG_MIN_CTAS
+#define ASCB_SEG_MIN_CTAS 6
+#endif
+
+template <typename T>
+struct SegSmem {
+  uint32_t bits[kItems / 32 + 1];  // row-start bitmap of positions 0..256
+  int rowid[33];                   // k-th nonempty row of the tile -> lane
+  int64_t bnd[kChunk + 1];         // first row of tiles c0 .. c0 + kChunk
+  T yinit[33];                     // exact standard form: y of the k-th row
+};
+
+// Arithmetic of the two modes.  EXACT rounds every product and sum separately
+// in the reference's order: compat s = +0 + v*x + ..., y = alpha*s + beta*y
+// (src/sparse/reference_blas.cc:13-39); standard s = y + (alpha*v)*x + ...
+// (include/asc/sparse/blas.h:1653-1665).  FAST forms plain sums.
+template <bool EXACT, bool STANDARD, typename T>
+__device__ __forceinline__ T product(T alpha, T v, T xv) {
+  if (EXACT && STANDARD) return mul_rn(mul_rn(alpha, v), xv);
+  return EXACT ? mul_rn(v, xv) : v * xv;
+}
+template <bool EXACT, typename T>
+__device__ __forceinline__ T add(T a, T b) {
+  return EXACT ? add_rn(a, b) : a + b;
+}
+template <bool EXACT, bool STANDARD, typename T>
+__device__ __forceinline__ T row_init(T y_old) {
+  return (EXACT && STANDARD) ? y_old : T(0);
+}
+
+template <typename T>
+__device__ __forceinline__ void load_vec2(const T* p, T& a, T& b);
+template <>
+__device__ __forceinline__ void load_vec2<double>(const double* p, double& a, double& b) {
+  const double2 v = __ldcs(reinterpret_cast<const double2*>(p));
+  a = v.x;
+  b = v.y;
+}
+__device__ __forceinline__ void load_idx2(const int64_t* p, int64_t& a, int64_t& b) {
+  const longlong2 v = __ldcs(reinterpret_cast<const longlong2*>(p));
+  a = v.x;
+  b = v.y;
+}
+
+template <bool EXACT, bool STANDARD, typename T>
+__device__ __forceinline__ T finish(T s, T alpha, T beta, const T* yp) {
+  if (EXACT) {
+    if (STANDARD) return s;
+    T r = mul_rn(alpha, s);
+    if (beta != T(0)) r = add_rn(r, mul_rn(beta, *yp));
+    return r;
+  }
+  if (STANDARD) return fma(alpha, s, *yp);
+  return beta != T(0) ? fma(alpha, s, beta * *yp) : alpha * s;
+}
+
+// Products of the lane's 8 positions, read from ip[0..8) / vp[0..8) (16-byte
+// aligned); bit k of vmask says whether position k holds a nonzero of the
+// window.  Invalid positions give 0.  16-byte chunks that are wholly valid are
+// fetched with one vector load, others element by element.
+template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+__device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
+                                              const int64_t* __restrict__ ip,
+                                              const T* __restrict__ vp, const T* __restrict__ x,
+                                              int64_t incx, T alpha) {
+  int64_t c[kPer];
+  T v[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; k += 2) {
+    if (((vmask >> k) & 3u) == 3u) {
+      load_idx2(ip + k, c[k], c[k + 1]);
+    } else {
+      c[k] = ((vmask >> k) & 1u) ? ld_stream(ip + k) : 0;
+      c[k + 1] = ((vmask >> (k + 1)) & 1u) ? ld_stream(ip + k + 1) : 0;
+    }
+  }
+  if constexpr (sizeof(T) == 8) {
+#pragma unroll
+    for (int k = 0; k < kPer; k += 2) {
+      if (((vmask >> k) & 3u) == 3u) {
+        load_vec2(vp + k, v[k], v[k + 1]);
+      } else {
+        v[k] = ((vmask >> k) & 1u) ? ld_stream(vp + k) : T(0);
+        v[k + 1] = ((vmask >> (k + 1)) & 1u) ? ld_stream(vp + k + 1) : T(0);
+      }
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < kPer; k += 4) {
+      if (((vmask >> k) & 15u) == 15u) {
+        const float4 f = __ldcs(reinterpret_cast<const float4*>(vp + k));
+        v[k] = f.x;
+        v[k + 1] = f.y;
+        v[k + 2] = f.z;
+        v[k + 3] = f.w;
+      } else {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          v[k + u] = ((vmask >> (k + u)) & 1u) ? ld_stream(vp + k + u) : T(0);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    p[k] = ((vmask >> k) & 1u)
+               ? product<EXACT, STANDARD>(alpha, v[k], ld_gather(&at<UNIT>(x, c[k], incx)))
+               : T(0);
+  }
+}
+
+template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+__global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
+seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
+           const T* __restrict__ val, const T* __restrict__ x, int64_t incx, T* __restrict__ y,
+           int64_t incy, T alpha, T beta, const int64_t* __restrict__ tile_row, int64_t ntiles,
+           int64_t rows, int64_t nnz) {
+  __shared__ SegSmem<T> smem_all[kWarpsPerCta];
+  const int lane = threadIdx.x & 31;
+  SegSmem<T>& w = smem_all[threadIdx.x >> 5];
+  const unsigned lt_mask = (1u << lane) - 1u;
+  // elements per 16-byte chunk of the narrower-aligned array
+  constexpr int64_t kAlign = sizeof(T) == 8 ? 2 : 4;
+
+  const int64_t warp_id = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + (threadIdx.x >> 5);
+  const int64_t warp_count = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
+  const int64_t per_warp = (ntiles + warp_count - 1) / warp_count;
+  const int64_t tb = warp_id * per_warp;
+  const int64_t te = tb + per_warp < ntiles ? tb + per_warp : ntiles;
+  if (tb >= te) return;
+
+  int64_t c0 = -2 * kChunk;
+  auto tile_bounds = [&](int64_t u, int64_t& r0, int& nr) {
+    if (u + 1 > c0 + kChunk) {
+      __syncwarp();
+      c0 = u;
+      for (int i = lane; i <= kChunk; i += 32) {
+        const int64_t v = c0 + i;
+        int64_t b = rows;
+        if (v < ntiles) {
+          b = tile_row != nullptr ? __ldg(tile_row + v)
+                                  : first_row_at(ptr, rows, kRowWeight, v * kItems);
+        }
+        w.bnd[i] = b;
+      }
+      __syncwarp();
+    }
+    r0 = w.bnd[u - c0];
+    nr = static_cast<int>(w.bnd[u - c0 + 1] - r0);
+  };
+
+  // prefetch of the next tile's row bounds (one round trip ahead)
+  int64_t r0_n;
+  int nr_n;
+  tile_bounds(tb, r0_n, nr_n);
+  int64_t rb_n = lane < nr_n ? __ldg(ptr + r0_n + lane) : 0;
+  int64_t re_n = lane < nr_n ? __ldg(ptr + r0_n + lane + 1) : 0;
+
+  for (int64_t t = tb; t < te; ++t) {
+    const int64_t r0 = r0_n;
+    const int nr = nr_n;
+    const int64_t rb = rb_n;
+    const int64_t re = re_n;
+    if (t + 1 < te) {
+      tile_bounds(t + 1, r0_n, nr_n);
+      rb_n = lane < nr_n ? __ldg(ptr + r0_n + lane) : 0;
+      re_n = lane < nr_n ? __ldg(ptr + r0_n + lane + 1) : 0;
+    }
+    if (nr == 0) continue;
+
+    const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
+    const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
+    const int64_t a0 = base / kAlign * kAlign;
+    const int lo = static_cast<int>(base - a0);
+    const int window = static_cast<int>(span < kItems - lo ? span : kItems - lo);
+    const int lim = lo + window;
+    const bool ends_here = span <= window;  // the last row ends in the window
+
+    // row-start bitmap (+ end marker at lim) and nonempty-row table
+    if (lane <= kItems / 32) w.bits[lane] = 0u;
+    __syncwarp();
+    const bool mine = lane < nr;
+    const bool nonempty = mine && re > rb;
+    if (nonempty) {
+      const int s = static_cast<int>(rb - a0);
+      atomicOr(&w.bits[s >> 5], 1u << (s & 31));
+    }
+    if (lane == 0 && ends_here) atomicOr(&w.bits[lim >> 5], 1u << (lim & 31));
+    const unsigned ne_mask = __ballot_sync(0xffffffffu, nonempty);
+    if (nonempty) {
+      const int k = __popc(ne_mask & lt_mask);
+      w.rowid[k] = lane;
+      if (EXACT && STANDARD) w.yinit[k] = at<UNIT>(y, r0 + lane, incy);
+    }
+    if (mine && !nonempty && !STANDARD) {  // empty row: y = alpha*(+0) + beta*y
+      T* yp = &at<UNIT>(y, r0 + lane, incy);
+      *yp = finish<EXACT, STANDARD>(T(0), alpha, beta, yp);
+    }
+    __syncwarp();
+
+    // lane's 8 contiguous positions [8*lane, 8*lane + 8) of the window
+    const int p0 = kPer * lane;
+    const int vlo = lo - p0 < 0 ? 0 : (lo - p0 > kPer ? kPer : lo - p0);
+    const int vhi = lim - p0 < 0 ? 0 : (lim - p0 > kPer ? kPer : lim - p0);
+    const uint32_t vmask = ((1u << vhi) - 1u) & ~((1u << vlo) - 1u);
+    T p[kPer];
+    lane_products<T, EXACT, STANDARD, UNIT>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
+                                            alpha);
+    const uint32_t word = w.bits[lane >> 2];
+    const uint32_t flags = (word >> ((lane & 3) * 8)) & 0xffu;
+    const uint32_t next_word = w.bits[(lane + 1) >> 2];
+    const bool next_start = ((next_word >> (((lane + 1) & 3) * 8)) & 1u) != 0u;
+    // segment ranks: starts strictly before this lane
+    int before = __popc(flags);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, before, o);
+      if (lane >= o) before += v;
+    }
+    before -= __popc(flags);  // exclusive
+
+    // local segmented sum.  A segment that starts inside the lane is summed
+    // here (in stored order); the lane's first segment, when it continues a
+    // row from earlier lanes, is joined below.
+    const bool has_data = vmask != 0u;
+    int rank = before;  // rows started at or before the current position
+    T acc = T(0);
+    bool first_seg = true;  // still in the segment open at the lane's start
+    T first_val = T(0);
+    int first_rank = -1;
+    int first_end = kPer;   // position where the continued segment closes
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      if ((flags >> i) & 1u) {
+        if (i > 0 && p0 + i > lo) {  // close the segment before position i
+          if (first_seg) {
+            first_val = acc;
+            first_rank = rank;
+            first_end = i;
+          } else {
+            T* yp = &at<UNIT>(y, r0 + w.rowid[rank - 1], incy);
+            *yp = finish<EXACT, STANDARD>(acc, alpha, beta, yp);
+          }
+        }
+        first_seg = false;
+        ++rank;
+        acc = add<EXACT>(row_init<EXACT, STANDARD>(w.yinit[rank - 1]), p[i]);
+      } else if (!(EXACT && first_seg)) {
+        acc = add<EXACT>(acc, p[i]);
+      }
+    }
+    const bool has_start = flags != 0u;
+    T c;  // this lane's carry out: the running sum of the row open at its end
+    T carry_in = T(0);
+    if (!EXACT) {
+      // segmented scan of the open tails: c = has_start ? acc : c_prev + acc
+      c = acc;
+      bool f = has_start;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const T cu = __shfl_up_sync(0xffffffffu, c, o);
+        const bool fu = __shfl_up_sync(0xffffffffu, f, o);
+        if (lane >= o) {
+          if (!f) c = cu + c;
+          f = f || fu;
+        }
+      }
+      carry_in = __shfl_up_sync(0xffffffffu, c, 1);
+      if (lane == 0) carry_in = T(0);
+      if (first_rank > 0) {  // continued row closed inside this lane
+        T* yp = &at<UNIT>(y, r0 + w.rowid[first_rank - 1], incy);
+        *yp = finish<EXACT, STANDARD>(carry_in + first_val, alpha, beta, yp);
+      }
+    } else {
+      // exact: the running sum is handed lane to lane; a lane whose first
+      // valid position starts a row (or that has no data) needs nothing.
+      bool resolved = !has_data || ((flags >> vlo) & 1u);
+      c = acc;
+      for (int step = 0; step < 32; ++step) {
+        const T cu = __shfl_up_sync(0xffffffffu, c, 1);
+        const bool ru = __shfl_up_sync(0xffffffffu, resolved, 1);
+        if (!resolved && ru) {
+          T s = cu;
+#pragma unroll
+          for (int k = 0; k < kPer; ++k) {
+            if (k >= vlo && k < first_end) s = add_rn(s, p[k]);
+          }
+          if (first_rank > 0) {
+            T* yp = &at<UNIT>(y, r0 + w.rowid[first_rank - 1], incy);
+            *yp = finish<EXACT, STANDARD>(s, alpha, beta, yp);
+            c = acc;
+          } else {
+            c = s;
+          }
+          resolved = true;
+        }
+        if (__all_sync(0xffffffffu, resolved)) break;
+      }
+    }
+    if (has_data && next_start && rank > 0 && p0 + kPer <= lim) {
+      // the open segment closes at the lane end (row start or data end next)
+      T* yp = &at<UNIT>(y, r0 + w.rowid[rank - 1], incy);
+      *yp = finish<EXACT, STANDARD>(c, alpha, beta, yp);
+    }
+    const T carry_out = __shfl_sync(0xffffffffu, c, 31);
+
+    if (!ends_here) {
+      // long last row: the nonzeros past the window
+      T total;
+      if (!EXACT) {
+        T part = T(0);
+        for (int64_t q = base + window + lane; q < base + span; q += 32) {
+          part = fma(ld_stream(val + q), ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)), part);
+        }
+#pragma unroll
+        for (int m = 16; m > 0; m >>= 1) part += shfl_xor(part, m);
+        total = carry_out + part;
+      } else {
+        // 32 products per round, then added in stored order
+        total = carry_out;
+        for (int64_t q0 = base + window; q0 < base + span; q0 += 32) {
+          const int64_t q = q0 + lane;
+          T pv = T(0);
+          if (q < base + span) {
+            pv = product<true, STANDARD>(alpha, ld_stream(val + q),
+                                         ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)));
+          }
+          const int n = static_cast<int>(base + span - q0 < 32 ? base + span - q0 : 32);
+          for (int k = 0; k < n; ++k) total = add_rn(total, __shfl_sync(0xffffffffu, pv, k));
+        }
+      }
+      if (lane == 0) {
+        T* yp = &at<UNIT>(y, r0 + nr - 1, incy);
+        *yp = finish<EXACT, STANDARD>(total, alpha, beta, yp);
+      }
+    }
+    __syncwarp();  // bitmap and row tables are rewritten by the next tile
+  }
+  (void)nnz;
+}
+
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, typename Kernel>
+int resident(Kernel kernel) {
+  static int cached[kMaxDevices] = {};
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return 1;
+  if (cached[device] == 0) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kThreads, 0) != cudaSuccess ||
+        n <= 0) {
+      (void)cudaGetLastError();
+      n = 1;
+    }
+    cached[device] = n;
+  }
+  return cached[device];
+}
+
+template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+int launch(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
+           const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count) {
+  auto kernel = seg_kernel<T, EXACT, STANDARD, UNIT>;
+  const int64_t warps_needed = (ntiles + 3) / 4;
+  const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
+  const int64_t resident_ctas =
+      static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * resident<T, EXACT, STANDARD, UNIT>(kernel);
+  const unsigned blocks = static_cast<unsigned>(
+      ctas_needed < 1 ? 1 : (ctas_needed < resident_ctas ? ctas_needed : resident_ctas));
+  kernel<<<blocks, kThreads, 0, stream>>>(
+      a->ptr, a->idx, static_cast<const T*>(a->val), static_cast<const T*>(x->data), x->stride,
+      static_cast<T*>(y->data), y->stride, alpha, beta, tile_row, ntiles, a->rows, a->nnz);
+  return static_cast<int>(cudaGetLastError());
+}
+
+template <typename T, bool EXACT>
+int by_form(cudaStream_t s, int form, const ascb_csr* a, double alpha, double beta,
+            const ascb_vec* x, const ascb_vec* y, const int64_t* tiles, int64_t n, int sm) {
+  const bool unit = x->stride == 1 && y->stride == 1;
+  const T al = static_cast<T>(alpha), be = static_cast<T>(beta);
+  if (form == ASCB_STANDARD) {
+    return unit ? launch<T, EXACT, true, true>(s, a, al, be, x, y, tiles, n, sm)
+                : launch<T, EXACT, true, false>(s, a, al, be, x, y, tiles, n, sm);
+  }
+  return unit ? launch<T, EXACT, false, true>(s, a, al, be, x, y, tiles, n, sm)
+              : launch<T, EXACT, false, false>(s, a, al, be, x, y, tiles, n, sm);
+}
+
+}  // namespace
+}  // namespace ascb
+
+extern "C" int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* a,
+                             double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
+                             const int64_t* tile_row, int64_t ntiles, int sm_count) {
+  if (ntiles <= 0) return 0;
+  auto s = static_cast<cudaStream_t>(stream);
+  if (dtype == ASCB_F64) {
+    return exact ? ascb::by_form<double, true>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count)
+                 : ascb::by_form<double, false>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count);
+  }
+  return exact ? ascb::by_form<float, true>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count)
+               : ascb::by_form<float, false>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count);
+}

@@ -40,7 +40,10 @@ constexpr int64_t kItems = 256;        // weighted items per tile
 constexpr int64_t kRowWeight = kItems / 32;
 constexpr int kPerLane = kItems / 32;  // staged products per lane
 constexpr int kChunk = 32;             // tile bounds cached per warp
-constexpr int kBatch = 4;              // gathers in flight per lane per batch
+#ifndef ASCB_WARP_BATCH
+#define ASCB_WARP_BATCH 4
+#endif
+constexpr int kBatch = ASCB_WARP_BATCH;  // gathers in flight per lane per batch
 #ifndef ASCB_WARP_MIN_CTAS
 #define ASCB_WARP_MIN_CTAS 6
 #endif
@@ -80,23 +83,24 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
-// Per-warp shared state.  FP64 products overwrite their own index slots (the
-// same lane reads index q and writes product q); FP32 products use `prod`.
+// Product q lives at padded slot pq(q) = q + q/16.  Rows summed one per lane
+// start at arbitrary offsets; with rows of 16 products the unpadded layout
+// put all 16 lanes of a half-warp on one bank.  The pad skews them apart,
+// while the staging writes (32 consecutive q) stay conflict-free.
+__device__ __forceinline__ int pq(int q) { return q + (q >> 4); }
+
+// Per-warp shared state.
 template <typename T>
 struct WarpSmem {
   int64_t ring[2][kItems];           // column indices, double buffered
   int64_t rows[3][kChunk + 1];       // ptr[r0 .. r0 + nr] per pipelined tile
   int64_t bnd[kChunk + 1];           // first row of tiles c0 .. c0 + kChunk
-  T prod[sizeof(T) == 8 ? 1 : kItems];
+  T prod[kItems + kItems / 16];      // products, padded layout
 };
 
 template <typename T>
-__device__ __forceinline__ T* products(WarpSmem<T>& w, int slot) {
-  if constexpr (sizeof(T) == 8) {
-    return reinterpret_cast<T*>(w.ring[slot]);
-  } else {
-    return w.prod;
-  }
+__device__ __forceinline__ T* products(WarpSmem<T>& w, int /*slot*/) {
+  return w.prod;
 }
 
 // Stage the products of nonzeros [first, first + count), count <= kItems,
@@ -122,7 +126,7 @@ __device__ __forceinline__ void stage(T* __restrict__ buf, int lane, int64_t fir
     for (int j = 0; j < kBatch; ++j) {
       const int q = (j0 + j) * 32 + lane;
       if (q < count) {
-        buf[q] = product<EXACT, STANDARD>(alpha, v[j], ld_gather(&at<UNIT>(x, col[j], incx)));
+        buf[pq(q)] = product<EXACT, STANDARD>(alpha, v[j], ld_gather(&at<UNIT>(x, col[j], incx)));
       }
     }
   }
@@ -229,7 +233,7 @@ warp_tile_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ id
         for (int j = 0; j < kBatch; ++j) {
           const int q = (j0 + j) * 32 + lane;
           if (q < count) {
-            buf[q] = product<EXACT, STANDARD>(alpha, v[j], ld_gather(&at<UNIT>(x, col[j], incx)));
+            buf[pq(q)] = product<EXACT, STANDARD>(alpha, v[j], ld_gather(&at<UNIT>(x, col[j], incx)));
           }
         }
       }
@@ -242,7 +246,7 @@ warp_tile_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ id
         const int64_t re = w.rows[k_cur][lane + 1] - base;
         s = STANDARD ? *yp : T(0);
         const int e = re < count ? static_cast<int>(re) : count;
-        for (int q = static_cast<int>(rb); q < e; ++q) s = add<EXACT>(s, buf[q]);
+        for (int q = static_cast<int>(rb); q < e; ++q) s = add<EXACT>(s, buf[pq(q)]);
         if (re <= count) *yp = finish<EXACT, STANDARD>(s, alpha, beta, yp);
       }
       if (span > kItems) {
@@ -254,11 +258,11 @@ warp_tile_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ id
           __syncwarp();
           if (EXACT) {
             if (lane == owner) {
-              for (int q = 0; q < n; ++q) s = add_rn(s, buf[q]);
+              for (int q = 0; q < n; ++q) s = add_rn(s, buf[pq(q)]);
             }
           } else {
             T part = T(0);
-            for (int q = lane; q < n; q += 32) part += buf[q];
+            for (int q = lane; q < n; q += 32) part += buf[pq(q)];
 #pragma unroll
             for (int m = 16; m > 0; m >>= 1) part += shfl_xor(part, m);
             if (lane == owner) s += part;
@@ -279,9 +283,9 @@ warp_tile_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ id
 // CTAs that fit on one SM at once (queried once per device and instantiation):
 // the grid is exactly one resident wave, so the static split of tiles over
 // warps is balanced.
-template <typename Kernel>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, typename Kernel>
 int resident_ctas_per_sm(Kernel kernel) {
-  static int cached[kMaxDevices] = {};
+  static int cached[kMaxDevices] = {};  // one cache per instantiation
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return 1;
   if (cached[device] == 0) {
@@ -304,7 +308,8 @@ int launch(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_v
   const int64_t warps_needed = (ntiles + 3) / 4;
   const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
   const int64_t resident =
-      static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * resident_ctas_per_sm(kernel);
+      static_cast<int64_t>(sm_count > 0 ? sm_count : 148) *
+      resident_ctas_per_sm<T, EXACT, STANDARD, UNIT>(kernel);
   const unsigned blocks = static_cast<unsigned>(
       ctas_needed < 1 ? 1 : (ctas_needed < resident ? ctas_needed : resident));
   kernel<<<blocks, kThreads, 0, stream>>>(

@@ -121,6 +121,13 @@ class SparseCudaContext:
     def launch_count(self) -> int:
         return int(self._lib.asc_sb_context_launch_count(self.handle))
 
+    def device_status(self, clear: bool = False) -> int:
+        """Nonzero if a kernel of this context gave up a bounded wait."""
+        v = ctypes.c_int32()
+        self.check(self._lib.asc_sb_context_device_status(self.handle, ctypes.byref(v),
+                                                          1 if clear else 0))
+        return v.value
+
 
 @dataclass
 class CudaCsrArray:

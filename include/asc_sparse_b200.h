@@ -172,6 +172,11 @@ ASC_SB_API int asc_sb_context_synchronize(asc_sb_context* context);
 ASC_SB_API const char* asc_sb_context_last_error(const asc_sb_context* context);
 /* Kernel launches issued by this context since creation (instrumentation). */
 ASC_SB_API int64_t asc_sb_context_launch_count(const asc_sb_context* context);
+/* Reads (and optionally clears) the context's device status word: nonzero
+ * means a kernel gave up a bounded wait and its results are not valid.
+ * Synchronizes the context stream. */
+ASC_SB_API int asc_sb_context_device_status(asc_sb_context* context,
+                                            int32_t* value, int32_t clear);
 
 /* ---- compat SpMV  y = alpha * A * x + beta * y ----------------------------- */
 

@@ -323,3 +323,124 @@ def test_failures_do_not_mutate(cuda_lib):
     assert e.value.code == ErrorCode.kInvalidState
     assert bits_equal(host(y), before)
     ctx.close()
+
+
+def _shapes(rng, dt):
+    lengths = np.array([1, 9000, 3, 20000, 0, 4097, 2047, 2049, 5000, 0, 0, 257, 255, 256] * 2)
+    ptr, idx = synthetic._unique_sorted_rows(rng, 30000, lengths)
+    long_rows = synthetic.Csr(lengths.size, 30000, ptr, idx,
+                              rng.standard_normal(int(ptr[-1])).astype(dt))
+    return {
+        "irregular": synthetic.random_csr(rng, 3000, 2500, 90, dt, 0.1),
+        "long_rows": long_rows,
+        "empty_rows": synthetic.random_csr(rng, 20000, 500, 6, dt, 0.9),
+        "power_law": synthetic.power_law(20000, seed=5, dtype=dt),
+        "single": synthetic.random_csr(rng, 1, 7, 7, dt),
+    }
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+def test_merge_variant_within_bound(cuda_lib, restatement, tag, dt):
+    """MERGE_PATH (contracted) stays inside the error bound on every shape."""
+    rng = np.random.default_rng(21)
+    ctx = context(Determinism.kBackendDefault)
+    ctx.set_variant(Variant.kMergePath)
+    for name, a_h in _shapes(rng, dt).items():
+        x_h = rng.uniform(-1, 1, a_h.cols).astype(dt)
+        y0 = rng.uniform(-1, 1, a_h.rows).astype(dt)
+        a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+        exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
+                                             a_h.val, x_h)
+        counts = np.diff(a_h.ptr)
+        for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
+            y = dev(y0)
+            compat(ctx, a, alpha, dev(x_h), beta, y)
+            ref = alpha * exact.astype(np.float64) + beta * y0.astype(np.float64)
+            assert_within_bound(host(y), exact, absval, counts, dt, alpha,
+                                np.abs(beta * y0.astype(np.float64)), ref)
+            y = dev(y0)
+            CudaSpmv(ctx, SparseBlasTranspose.kNone, alpha, a, vec(dev(x_h), writable=False),
+                     vec(y))
+            ref = y0.astype(np.float64) + alpha * exact.astype(np.float64)
+            assert_within_bound(host(y), exact, absval, counts, dt, alpha,
+                                np.abs(y0.astype(np.float64)), ref)
+    assert ctx.device_status() == 0
+    ctx.close()
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("misalign", [False, True])
+def test_warp_tiles_variant_within_bound(cuda_lib, restatement, tag, dt, misalign):
+    """WARP_TILES (register-segmented kernel; scalar-load kernel when the
+    arrays are not 16-byte aligned) stays inside the error bound."""
+    rng = np.random.default_rng(23)
+    ctx = context(Determinism.kBackendDefault)
+    ctx.set_variant(Variant.kWarpTiles)
+    for name, a_h in _shapes(rng, dt).items():
+        x_h = rng.uniform(-1, 1, a_h.cols).astype(dt)
+        y0 = rng.uniform(-1, 1, a_h.rows).astype(dt)
+        a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+        if misalign:  # idx/val views starting 8 (resp. 4) bytes into a buffer
+            idx_store = torch.zeros(a_h.nnz + 1, dtype=torch.int64, device="cuda")
+            val_store = torch.zeros(a_h.nnz + 1, dtype=a.values.dtype, device="cuda")
+            idx_store[1:] = a.indices
+            val_store[1:] = a.values
+            a.indices, a.values = idx_store[1:], val_store[1:]
+        exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
+                                             a_h.val, x_h)
+        counts = np.diff(a_h.ptr)
+        for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
+            y = dev(y0)
+            compat(ctx, a, alpha, dev(x_h), beta, y)
+            ref = alpha * exact.astype(np.float64) + beta * y0.astype(np.float64)
+            assert_within_bound(host(y), exact, absval, counts, dt, alpha,
+                                np.abs(beta * y0.astype(np.float64)), ref)
+            y = dev(y0)
+            CudaSpmv(ctx, SparseBlasTranspose.kNone, alpha, a, vec(dev(x_h), writable=False),
+                     vec(y))
+            ref = y0.astype(np.float64) + alpha * exact.astype(np.float64)
+            assert_within_bound(host(y), exact, absval, counts, dt, alpha,
+                                np.abs(y0.astype(np.float64)), ref)
+    ctx.close()
+
+
+@pytest.mark.parametrize("tag,dt", DTYPES)
+@pytest.mark.parametrize("misalign", [False, True])
+def test_exact_paths_bit_exact_on_all_shapes(cuda_lib, restatement, tag, dt, misalign):
+    """Deterministic mode through every route: workspace partition, no
+    partition (in-kernel tile search), plan; 16-byte aligned arrays take the
+    register-segmented kernel, misaligned ones the scalar-load warp kernel."""
+    rng = np.random.default_rng(22)
+    ctx = context()
+    for name, a_h in _shapes(rng, dt).items():
+        x_h = rng.uniform(-1, 1, a_h.cols).astype(dt)
+        y0 = rng.uniform(-1, 1, a_h.rows).astype(dt)
+        a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+        if misalign:
+            idx_store = torch.zeros(a_h.nnz + 1, dtype=torch.int64, device="cuda")
+            val_store = torch.zeros(a_h.nnz + 1, dtype=a.values.dtype, device="cuda")
+            idx_store[1:] = a.indices
+            val_store[1:] = a.values
+            a.indices, a.values = idx_store[1:], val_store[1:]
+        expect = y0.copy()
+        restatement.compat_spmv(a_h.ptr, a_h.idx, a_h.val, 1.25, x_h, -0.5, expect)
+        y = dev(y0)
+        compat(ctx, a, 1.25, dev(x_h), -0.5, y)
+        assert bits_equal(host(y), expect), name
+        plan = CsrPlan(ctx, a)
+        y = dev(y0)
+        plan.csr_spmv(1.25, vec(dev(x_h), writable=False), -0.5, vec(y))
+        assert bits_equal(host(y), expect), name
+        expect_std = y0.copy()
+        restatement.standard_spmv(CSR, OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val,
+                                  -2.0, x_h, expect_std)
+        y = dev(y0)
+        CudaSpmv(ctx, SparseBlasTranspose.kNone, -2.0, a, vec(dev(x_h), writable=False), vec(y),
+                 plan=plan)
+        assert bits_equal(host(y), expect_std), name
+        y = dev(y0)
+        CudaSpmv(ctx, SparseBlasTranspose.kNone, -2.0, a, vec(dev(x_h), writable=False), vec(y))
+        assert bits_equal(host(y), expect_std), name
+        plan.close()
+    assert ctx.device_status() == 0
+    ctx.close()
