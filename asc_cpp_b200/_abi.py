@@ -141,6 +141,7 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_context_device_status": (ctypes.c_int, [_P, ctypes.POINTER(_I32), _I32]),
     "asc_sb_csr_spmv_workspace_size": (ctypes.c_int, [_P, _SP, _VP, _VP, ctypes.POINTER(_SZ)]),
     "asc_sb_csr_spmv": (ctypes.c_int, [_P, _D, _SP, _VP, _D, _VP, _P, _SZ, _I32]),
+    "asc_sb_csr_spmv_no_alloc": (ctypes.c_int, [_P, _D, _SP, _VP, _D, _VP]),
     "asc_sb_standard_spmv": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _VP, _VP]),
     "asc_sb_standard_spmm": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _DP, _DP]),
     "asc_sb_plan_workspace_size": (ctypes.c_int, [_P, _SP, _I32, ctypes.POINTER(_SZ)]),

@@ -16,6 +16,7 @@
 
 #include "../../../include/asc_sparse_b200.h"
 #include "../kernels.h"
+#include "context_view.h"
 #include "validate.h"
 
 using ascb::host::Fail;
@@ -729,3 +730,19 @@ int asc_sb_plan_standard_spmv(asc_sb_context* ctx, const asc_sb_plan* plan, int3
 }
 
 }  // extern "C"
+
+namespace ascb::host {
+
+bool ViewContext(asc_sb_context* ctx, ContextView* view) {
+  if (ctx == nullptr || view == nullptr) return false;
+  view->device = ctx->device;
+  view->stream = ctx->stream;
+  view->determinism = ctx->determinism;
+  view->sm_count = ctx->sm_count;
+  view->mutex = &ctx->mutex;
+  view->last_error = &ctx->last_error;
+  view->launches = &ctx->launches;
+  return true;
+}
+
+}  // namespace ascb::host

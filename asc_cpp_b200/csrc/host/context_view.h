@@ -1,0 +1,28 @@
+// Read access to a context's fields for entry points defined outside api.cc.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+#include "../../../include/asc_sparse_b200.h"
+
+namespace ascb::host {
+
+struct ContextView {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  int determinism = ASC_SB_DETERMINISTIC;
+  int sm_count = 148;
+  std::mutex* mutex = nullptr;
+  std::string* last_error = nullptr;
+  std::atomic<std::int64_t>* launches = nullptr;
+};
+
+// False for a null context.
+bool ViewContext(asc_sb_context* context, ContextView* view);
+
+}  // namespace ascb::host

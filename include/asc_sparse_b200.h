@@ -202,6 +202,23 @@ ASC_SB_API int asc_sb_csr_spmv(asc_sb_context* context, double alpha,
                                size_t workspace_bytes,
                                int32_t workspace_space);
 
+/* Compat SpMV that allocates nothing and takes no workspace.  No counterpart
+ * in the reference: it is for callers that cannot allocate device memory when
+ * they need the product -- code running during CUDA graph capture, plugin
+ * hosts that forbid device allocations outside their own allocator, and
+ * latency-critical loops that must not risk the device synchronisation of a
+ * cudaMalloc/cudaFree.  Same contract and results as asc_sb_csr_spmv with the
+ * context's determinism.  Its only scratch, the row-tile partition, is a
+ * static 2 MiB device array per GPU (held until the process exits): matrices
+ * needing more than 262,144 tile bounds -- ceil((8*rows + nnz)/256) + 1 --
+ * are rejected with ASC_SB_UNSUPPORTED.  All calls on a device share that
+ * array: calls that overlap on the GPU race.  The first call on each device
+ * looks up the array's address; make it before any stream capture. */
+ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, double alpha,
+                                        const asc_sb_sparse* matrix,
+                                        const asc_sb_vector* input, double beta,
+                                        const asc_sb_vector* output);
+
 /* ---- standard SpMV / SpMM  y += alpha * op(A) * x -------------------------- */
 
 /* Replaces internal_sparse_cuda::StandardSpmvErased (cuda.h:243-246;
