@@ -55,7 +55,7 @@ def _peaks():
 
 
 def _traffic_record():
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+    path = os.path.join(ROOT, "profiles", "seg_kernel_fp64_powerlaw_4M_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
             return json.load(f)
@@ -148,6 +148,25 @@ def run_reference(args, rank, world):
         rs = Restatement()
         run = lambda y: rs.compat_spmv(a.ptr, a.idx, a.val, 1.0, x, 0.0, y)  # noqa: E731
     y = np.zeros(a.rows)
+    sample = "full matrix"
+    bytes_ = a.bytes_spmv(8)
+    t0 = time.perf_counter()
+    run(y)
+    t_full = time.perf_counter() - t0
+    # keep the whole run within about two minutes: if K full products would
+    # take longer, each step runs the reference on a leading row block
+    budget = 120.0 / max(1, args.steps + args.warmup)
+    if t_full > budget:
+        rows = max(1, int(a.rows * budget / t_full))
+        nnz = int(a.ptr[rows])
+        sub_ptr, sub_idx, sub_val = a.ptr[:rows + 1], a.idx[:nnz], a.val[:nnz]
+        bytes_ = nnz * 16 + (rows + 1) * 8 + a.cols * 8 + rows * 8
+        sample = f"first {rows} rows ({nnz} nnz) per step"
+        if kind == "reference":
+            ref.blocks_free(handle, np.float64)
+            handle = ref.blocks_prepare(rows, a.cols, sub_ptr, sub_idx, sub_val, threads)
+        else:
+            run = lambda y: rs.compat_spmv(sub_ptr, sub_idx, sub_val, 1.0, x, 0.0, y)  # noqa: E731
     for _ in range(args.warmup):
         run(y)
     times = []
@@ -155,7 +174,6 @@ def run_reference(args, rank, world):
         t0 = time.perf_counter()
         run(y)
         times.append(time.perf_counter() - t0)
-    bytes_ = a.bytes_spmv(8)
     ms = 1e3 * statistics.mean(times)
     gbs = bytes_ / (ms * 1e-3) / 1e9
     line = {
@@ -167,8 +185,8 @@ def run_reference(args, rank, world):
                    "alpha": 1.0, "beta": 0.0, "bytes_per_step": bytes_},
         "cpu_baseline": {"value": round(gbs, 3), "unit": "GB/s", "cores": threads,
                          "kind": kind,
-                         "sample": "full matrix, one reference SpmvReference call per "
-                                   "nnz-balanced row block per thread"},
+                         "sample": sample + ", one reference SpmvReference call per "
+                                            "nnz-balanced row block per thread"},
         "e2e": {"value": round(gbs, 3), "unit": "GB/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -257,20 +275,33 @@ def run_gpu(args, rank, world):
     def run_plan():
         plan.csr_spmv(1.0, xv, 0.0, yv)
 
-    ctx.set_determinism(Determinism.kDeterministic)
-    detail["row_ordered_bitexact"] = bytes_step / (timed(run_plan, 5, 2) * 1e-3) / 1e9
-    ctx.set_determinism(Determinism.kBackendDefault)
-    for lanes in (2, 4, 8, 16):
-        ctx.set_variant(Variant.kVector, lanes)
-        detail[f"vector_{lanes}"] = bytes_step / (timed(run_plan, 5, 2) * 1e-3) / 1e9
+    # every variant once (untimed selection pass); the fastest is the headline
+    choices = {"row_ordered_bitexact": (Determinism.kDeterministic, Variant.kAuto, 0),
+               "warp_tiles": (Determinism.kBackendDefault, Variant.kWarpTiles, 0),
+               "merge_path": (Determinism.kBackendDefault, Variant.kMergePath, 0),
+               "vector_8": (Determinism.kBackendDefault, Variant.kVector, 8),
+               "vector_16": (Determinism.kBackendDefault, Variant.kVector, 16)}
+    if args.probe:
+        # profiling aid: a few launches of one variant, nothing timed
+        det, var, lanes = choices[args.probe]
+        ctx.set_determinism(det)
+        ctx.set_variant(var, lanes)
+        for _ in range(3):
+            run_plan()
+        stream.synchronize()
+        plan.close()
+        ctx.close()
+        return None
+    for name, (det, var, lanes) in choices.items():
+        ctx.set_determinism(det)
+        ctx.set_variant(var, lanes)
+        detail[name] = bytes_step / (timed(run_plan, 5, 2) * 1e-3) / 1e9
     best = max(detail, key=detail.get)
-    if best == "row_ordered_bitexact":
-        ctx.set_determinism(Determinism.kDeterministic)
-        mode = "deterministic (bit-exact row-ordered)"
-    else:
-        ctx.set_determinism(Determinism.kBackendDefault)
-        ctx.set_variant(Variant.kVector, int(best.split("_")[1]))
-        mode = f"backend_default ({best})"
+    det, var, lanes = choices[best]
+    ctx.set_determinism(det)
+    ctx.set_variant(var, lanes)
+    mode = ("deterministic (bit-exact)" if det == Determinism.kDeterministic
+            else f"backend_default ({best}, within gamma bound)")
 
     # -- headline: device-resident inputs --
     launches0 = ctx.launch_count
@@ -330,9 +361,11 @@ def run_gpu(args, rank, world):
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--probe", default=None,
+                   help="profiling aid: run 3 launches of one variant and exit")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = _env_int("RANK", 0)
