@@ -221,9 +221,10 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
   // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) run the register-
   // segmented kernel, which needs 16-byte aligned index and value arrays;
   // otherwise the scalar-load warp kernel with the same numerics.
-  const bool aligned16 =
-      ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) & 15u) == 0;
-  if (aligned16) {
+  const bool seg_aligned =
+      ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
+       static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
+  if (seg_aligned) {
     return Launched(ctx,
                     ascb_spmv_seg(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
                                   tiles_ptr, tiles, ctx->sm_count),

@@ -62,7 +62,9 @@ int ascb_spmv_merge(void* stream, int dtype, int form, int exact, const ascb_csr
                     double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
                     const int64_t* bounds, int64_t ntiles, int sm_count, int* status);
 // Register-segmented SpMV over the warp row tiles (exact = 1: bit-exact);
-// requires the column-index and value arrays to start on 16-byte boundaries.
+// requires the column-index and value arrays to start on
+// ascb_spmv_seg_alignment()-byte boundaries.
+int ascb_spmv_seg_alignment(void);
 int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
                   double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
                   int64_t ntiles, int sm_count);

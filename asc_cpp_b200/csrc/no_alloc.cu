@@ -155,9 +155,10 @@ extern "C" ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, doub
   int rc = ascb_row_tiles(v.stream, &a, items, weight, scratch, tiles);
   v.launches->fetch_add(1, std::memory_order_relaxed);
   if (rc == 0) {
-    const bool aligned16 =
-        ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) & 15u) == 0;
-    rc = aligned16 ? ascb_spmv_seg(v.stream, dtype, ASCB_COMPAT, exact, &a, alpha, beta, &xv, &yv,
+    const bool seg_aligned =
+        ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
+         static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
+    rc = seg_aligned ? ascb_spmv_seg(v.stream, dtype, ASCB_COMPAT, exact, &a, alpha, beta, &xv, &yv,
                                    scratch, tiles, v.sm_count)
                    : ascb_spmv_warp(v.stream, dtype, ASCB_COMPAT, exact, &a, alpha, beta, &xv, &yv,
                                     scratch, tiles, v.sm_count);

@@ -436,3 +436,5 @@ extern "C" int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const
   return exact ? ascb::by_form<float, true>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count)
                : ascb::by_form<float, false>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count);
 }
+
+extern "C" int ascb_spmv_seg_alignment(void) { return 16; }
