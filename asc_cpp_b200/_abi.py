@@ -122,6 +122,7 @@ class DenseDesc(ctypes.Structure):
 
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
 _D = ctypes.c_double
 _SZ = ctypes.c_size_t
 _SP = ctypes.POINTER(SparseDesc)
@@ -150,6 +151,12 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_destroy": (ctypes.c_int, [_P]),
     "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
     "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
+    "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
+    "asc_sb_convert_workspace_size": (ctypes.c_int, [_P, _I64, _I64, _I64, _I32,
+                                                     ctypes.POINTER(_SZ)]),
+    "asc_sb_convert_compressed": (ctypes.c_int, [_P, _SP, _SP, _P, _SZ]),
+    "asc_sb_convert_coordinates": (ctypes.c_int, [_P, _P, _P, _I32, _I64, _I64, _I64, _SP,
+                                                  _P, _SZ]),
 }
 
 _lib: ctypes.CDLL | None = None

@@ -258,6 +258,66 @@ std::size_t PartitionBytes(std::int64_t rows, std::int64_t nnz) {
   return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz);
 }
 
+std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
+  return RoundUp(static_cast<std::size_t>(nnz > 0 ? nnz : 1) * element, 256);
+}
+
+// Layout of a plan's workspace.  Without ASC_SB_PLAN_TRANSPOSE it holds the
+// partitions of the stored arrays only.  With it, also the transposed
+// structure (offsets, indices, the permutation that maps its entries to the
+// stored ones, and its values), that structure's partitions, and the scratch
+// the stable sort uses while the plan is created.
+struct PlanLayout {
+  std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, t_part = 0;
+  std::size_t sort = 0, outer_of = 0, total = 0;
+};
+
+PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
+  const bool csc = m.format == ASC_SB_CSC;
+  const std::int64_t outer = csc ? m.columns : m.rows;
+  const std::int64_t inner = csc ? m.rows : m.columns;
+  const std::int64_t nnz = m.nonzeros;
+  PlanLayout l;
+  std::size_t at = PartitionBytes(outer, nnz);
+  if (flags & ASC_SB_PLAN_TRANSPOSE) {
+    l.t_ptr = at;
+    at += RoundUp(static_cast<std::size_t>(inner + 1) * 8, 256);
+    l.t_idx = at;
+    at += EntryBytes(nnz, 8);
+    l.t_perm = at;
+    at += EntryBytes(nnz, 8);
+    l.t_val = at;
+    at += EntryBytes(nnz, ascb::host::ElementBytes(m.element_kind));
+    l.t_part = at;
+    at += PartitionBytes(inner, nnz);
+    l.sort = at;
+    at += RoundUp(ascb_sort_workspace_bytes(nnz, inner), 256);
+    l.outer_of = at;
+    at += EntryBytes(nnz, 8);
+  }
+  l.total = at;
+  return l;
+}
+
+// Stable transposed structure of the CSR arrays `a` (rows = stored outer
+// extent): t_ptr [a.cols + 1], t_idx / t_perm / t_val [nnz].
+Status BuildTransposed(asc_sb_context* ctx, const ascb_csr& a, std::size_t element,
+                       std::int64_t* t_ptr, std::int64_t* t_idx, std::int64_t* t_perm,
+                       void* t_val, void* sort_scratch, std::int64_t* outer_of) {
+  Status s = Launched(ctx,
+                      ascb_stable_sort(ctx->stream, a.idx, 1, a.nnz, a.cols, t_ptr, t_perm,
+                                       sort_scratch),
+                      "CUDA could not launch the transposition sort");
+  if (!s.ok()) return s;
+  s = Launched(ctx, ascb_outer_of_entries(ctx->stream, a.ptr, a.rows, outer_of, ctx->sm_count),
+               "CUDA could not launch the row expansion kernel");
+  if (!s.ok()) return s;
+  return Launched(ctx,
+                  ascb_permute_entries(ctx->stream, t_perm, a.nnz, outer_of, 1, t_idx, a.val,
+                                       t_val, static_cast<int>(element), ctx->sm_count),
+                  "CUDA could not launch the entry permutation kernel");
+}
+
 struct CompatOperands {
   SparseBytes matrix_bytes;
   Span x_span, y_span;
@@ -528,6 +588,19 @@ Status ValidateStandardSpmv(asc_sb_context* ctx, int op, double alpha_imag,
   return Status::Ok();
 }
 
+// The plan's transposed structure as CSR arrays (rows = stored inner extent).
+ascb_csr TransposedCsr(const asc_sb_plan& plan) {
+  const ascb_csr a = AsCsr(plan.matrix, plan.matrix.format == ASC_SB_CSC);
+  ascb_csr t{};
+  t.rows = a.cols;
+  t.cols = a.rows;
+  t.nnz = a.nnz;
+  t.ptr = plan.t_ptr;
+  t.idx = plan.t_idx;
+  t.val = plan.t_val;
+  return t;
+}
+
 // Runs y += alpha * op(A) x.  The stored arrays are read as a CSR matrix `a`
 // (for CSC: the CSR of A^T); `transposed` says whether the product needs the
 // transpose of those arrays.
@@ -545,13 +618,7 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
                   plan != nullptr ? &plan->part : nullptr);
   }
   if (plan != nullptr && plan->t_ptr != nullptr) {
-    ascb_csr t{};
-    t.rows = a.cols;
-    t.cols = a.rows;
-    t.nnz = a.nnz;
-    t.ptr = plan->t_ptr;
-    t.idx = plan->t_idx;
-    t.val = plan->t_val;
+    const ascb_csr t = TransposedCsr(*plan);
     const Choice choice = Choose(ctx, m);
     return RunCsr(ctx, choice, ASCB_STANDARD, t, dtype, alpha, 0.0, xv, yv, nullptr,
                   &plan->t_part);
@@ -582,6 +649,61 @@ int asc_sb_standard_spmv(asc_sb_context* ctx, int32_t op, double alpha_real, dou
 }
 
 // ---------------------------------------------------------------------------
+namespace {
+
+// C += alpha * op(A) * B, validated in full before anything is enqueued.  With
+// a plan that holds the transposed structure, a transposed product runs the
+// stored-order kernel on that structure (bit-exact); without one it scatters.
+Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double alpha_real,
+                    double alpha_imag, const asc_sb_sparse* m, const asc_sb_dense* b,
+                    const asc_sb_dense* c) {
+  if (op != ASC_SB_OP_NONE && op != ASC_SB_OP_TRANSPOSE && op != ASC_SB_OP_CONJUGATE_TRANSPOSE) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS transpose mode is invalid");
+  }
+  if (m == nullptr || b == nullptr || c == nullptr) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "CUDA SpMM descriptors cannot be null");
+  }
+  SparseBytes mb;
+  Status s = ascb::host::ValidateSparse(*m, ctx->device, &mb);
+  if (!s.ok()) return s;
+  if (!RealKind(m->element_kind) || alpha_imag != 0.0) {
+    return Fail(ASC_SB_UNSUPPORTED, "CUDA standardized SpMM supports real float and double");
+  }
+  Span bs, cs;
+  s = ascb::host::ValidateDense(*b, m->element_kind, false, ctx->device, &bs);
+  if (!s.ok()) return s;
+  s = ascb::host::ValidateDense(*c, m->element_kind, true, ctx->device, &cs);
+  if (!s.ok()) return s;
+  const std::int64_t inner = op == ASC_SB_OP_NONE ? m->columns : m->rows;
+  const std::int64_t rows = op == ASC_SB_OP_NONE ? m->rows : m->columns;
+  if (b->rows != inner || c->rows != rows || b->columns != c->columns) {
+    return Fail(ASC_SB_SHAPE, "CUDA standardized SpMM matrix extents do not match");
+  }
+  if (ascb::host::Overlap(bs, cs) || ascb::host::Overlap({m->structure_first, mb.first}, cs) ||
+      ascb::host::Overlap({m->structure_second, mb.second}, cs) ||
+      ascb::host::Overlap({m->values, mb.values}, cs)) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "CUDA standardized SpMM output overlaps an input");
+  }
+  if (alpha_real == 0.0 || c->rows == 0 || c->columns == 0) return Status::Ok();
+  const bool csc = m->format == ASC_SB_CSC;
+  const bool transposed = (op != ASC_SB_OP_NONE) != csc;
+  const bool planned = transposed && plan != nullptr && plan->t_ptr != nullptr;
+  if (transposed && !planned && ctx->determinism == ASC_SB_DETERMINISTIC) {
+    return Fail(ASC_SB_INVALID_STATE,
+                "A deterministic transposed SpMM needs a plan created with "
+                "ASC_SB_PLAN_TRANSPOSE");
+  }
+  const ascb_csr a = planned ? TransposedCsr(*plan) : AsCsr(*m, csc);
+  return Launched(ctx,
+                  ascb_spmm(ctx->stream, Dtype(m->element_kind), transposed && !planned ? 1 : 0,
+                            &a, c->columns, b->data, b->layout, b->leading_dimension,
+                            const_cast<void*>(c->data), c->layout, c->leading_dimension,
+                            alpha_real, ctx->sm_count),
+                  "CUDA could not launch the SpMM kernel");
+}
+
+}  // namespace
+
 int asc_sb_standard_spmm(asc_sb_context* ctx, int32_t op, double alpha_real, double alpha_imag,
                          const asc_sb_sparse* m, const asc_sb_dense* b, const asc_sb_dense* c) {
   Status s = ValidateContext(ctx);
@@ -589,48 +711,7 @@ int asc_sb_standard_spmm(asc_sb_context* ctx, int32_t op, double alpha_real, dou
   std::lock_guard<std::mutex> lock(ctx->mutex);
   DeviceGuard guard(ctx->device);
   if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
-  if (op != ASC_SB_OP_NONE && op != ASC_SB_OP_TRANSPOSE && op != ASC_SB_OP_CONJUGATE_TRANSPOSE) {
-    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS transpose mode is invalid"));
-  }
-  if (m == nullptr || b == nullptr || c == nullptr) {
-    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "CUDA SpMM descriptors cannot be null"));
-  }
-  SparseBytes mb;
-  s = ascb::host::ValidateSparse(*m, ctx->device, &mb);
-  if (!s.ok()) return Finish(ctx, s);
-  if (!RealKind(m->element_kind) || alpha_imag != 0.0) {
-    return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "CUDA standardized SpMM supports real float and double"));
-  }
-  Span bs, cs;
-  s = ascb::host::ValidateDense(*b, m->element_kind, false, ctx->device, &bs);
-  if (!s.ok()) return Finish(ctx, s);
-  s = ascb::host::ValidateDense(*c, m->element_kind, true, ctx->device, &cs);
-  if (!s.ok()) return Finish(ctx, s);
-  const std::int64_t inner = op == ASC_SB_OP_NONE ? m->columns : m->rows;
-  const std::int64_t rows = op == ASC_SB_OP_NONE ? m->rows : m->columns;
-  if (b->rows != inner || c->rows != rows || b->columns != c->columns) {
-    return Finish(ctx, Fail(ASC_SB_SHAPE, "CUDA standardized SpMM matrix extents do not match"));
-  }
-  if (ascb::host::Overlap(bs, cs) || ascb::host::Overlap({m->structure_first, mb.first}, cs) ||
-      ascb::host::Overlap({m->structure_second, mb.second}, cs) ||
-      ascb::host::Overlap({m->values, mb.values}, cs)) {
-    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "CUDA standardized SpMM output overlaps an input"));
-  }
-  if (alpha_real == 0.0 || c->rows == 0 || c->columns == 0) return Finish(ctx, Status::Ok());
-  const bool csc = m->format == ASC_SB_CSC;
-  const bool transposed = (op != ASC_SB_OP_NONE) != csc;
-  if (transposed && ctx->determinism == ASC_SB_DETERMINISTIC) {
-    return Finish(ctx, Fail(ASC_SB_INVALID_STATE,
-                            "A deterministic transposed SpMM needs the transposed structure "
-                            "(a CSR copy of A^T)"));
-  }
-  const ascb_csr a = AsCsr(*m, csc);
-  s = Launched(ctx,
-               ascb_spmm(ctx->stream, Dtype(m->element_kind), transposed ? 1 : 0, &a, c->columns,
-                         b->data, b->layout, b->leading_dimension, const_cast<void*>(c->data),
-                         c->layout, c->leading_dimension, alpha_real, ctx->sm_count),
-               "CUDA could not launch the SpMM kernel");
-  return Finish(ctx, s);
+  return Finish(ctx, StandardSpmm(ctx, nullptr, op, alpha_real, alpha_imag, m, b, c));
 }
 
 // ---------------------------------------------------------------------------
@@ -641,11 +722,13 @@ int asc_sb_plan_workspace_size(asc_sb_context* ctx, const asc_sb_sparse* m, int3
   if (m == nullptr || bytes == nullptr) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "plan arguments cannot be null"));
   }
-  if (flags & ASC_SB_PLAN_TRANSPOSE) {
-    return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "transposed plans are not built yet"));
+  if ((flags & ~ASC_SB_PLAN_TRANSPOSE) != 0) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "unknown plan flags"));
   }
-  const std::int64_t outer = m->format == ASC_SB_CSC ? m->columns : m->rows;
-  *bytes = PartitionBytes(outer, m->nonzeros);
+  if (m->rows < 0 || m->columns < 0 || m->nonzeros < 0) {
+    return Finish(ctx, Fail(ASC_SB_SHAPE, "plan matrix extents cannot be negative"));
+  }
+  *bytes = PlanLayoutFor(*m, flags).total;
   return Finish(ctx, Status::Ok());
 }
 
@@ -677,7 +760,19 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
   plan->flags = flags;
   const bool csc = m->format == ASC_SB_CSC;
   const ascb_csr a = AsCsr(*m, csc);
-  s = BuildPartitions(ctx, a, static_cast<unsigned char*>(workspace), &plan->part);
+  auto* ws = static_cast<unsigned char*>(workspace);
+  s = BuildPartitions(ctx, a, ws, &plan->part);
+  if (s.ok() && (flags & ASC_SB_PLAN_TRANSPOSE)) {
+    const PlanLayout l = PlanLayoutFor(*m, flags);
+    plan->t_ptr = reinterpret_cast<std::int64_t*>(ws + l.t_ptr);
+    plan->t_idx = reinterpret_cast<std::int64_t*>(ws + l.t_idx);
+    plan->t_perm = reinterpret_cast<std::int64_t*>(ws + l.t_perm);
+    plan->t_val = ws + l.t_val;
+    s = BuildTransposed(ctx, a, ascb::host::ElementBytes(m->element_kind), plan->t_ptr,
+                        plan->t_idx, plan->t_perm, plan->t_val, ws + l.sort,
+                        reinterpret_cast<std::int64_t*>(ws + l.outer_of));
+    if (s.ok()) s = BuildPartitions(ctx, TransposedCsr(*plan), ws + l.t_part, &plan->t_part);
+  }
   if (!s.ok()) {
     delete plan;
     return Finish(ctx, s);
@@ -689,7 +784,18 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
 int asc_sb_plan_refresh_values(asc_sb_context* ctx, asc_sb_plan* plan) {
   if (ctx == nullptr) return ASC_SB_INVALID_STATE;
   if (plan == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "null plan"));
-  return Finish(ctx, Status::Ok());
+  if (plan->t_ptr == nullptr) return Finish(ctx, Status::Ok());
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  // the transposed values are a gather of the stored ones through t_perm
+  return Finish(ctx, Launched(ctx,
+                              ascb_permute_entries(
+                                  ctx->stream, plan->t_perm, plan->matrix.nonzeros, nullptr, 0,
+                                  nullptr, plan->matrix.values, plan->t_val,
+                                  static_cast<int>(ascb::host::ElementBytes(plan->matrix.element_kind)),
+                                  ctx->sm_count),
+                              "CUDA could not launch the entry permutation kernel"));
 }
 
 int asc_sb_plan_destroy(asc_sb_plan* plan) {
@@ -728,6 +834,208 @@ int asc_sb_plan_standard_spmv(asc_sb_context* ctx, const asc_sb_plan* plan, int3
   if (!s.ok()) return Finish(ctx, s);
   if (alpha_real == 0.0 || y->extent == 0) return Finish(ctx, Status::Ok());
   return Finish(ctx, RunStandardSpmv(ctx, plan, plan->matrix, op, alpha_real, *x, *y));
+}
+
+int asc_sb_plan_standard_spmm(asc_sb_context* ctx, const asc_sb_plan* plan, int32_t op,
+                              double alpha_real, double alpha_imag, const asc_sb_dense* b,
+                              const asc_sb_dense* c) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "null plan"));
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  return Finish(ctx, StandardSpmm(ctx, plan, op, alpha_real, alpha_imag, &plan->matrix, b, c));
+}
+
+// ---------------------------------------------------------------------------
+// Format conversion on the device.
+
+namespace {
+
+struct ConvertLayout {
+  std::size_t perm = 0, outer_of = 0, sort = 0, total = 0;
+};
+
+ConvertLayout ConvertLayoutFor(std::int64_t nnz, std::int64_t destination_outer) {
+  ConvertLayout l;
+  std::size_t at = 0;
+  l.perm = at;
+  at += EntryBytes(nnz, 8);
+  l.outer_of = at;
+  at += EntryBytes(nnz, 8);
+  l.sort = at;
+  at += RoundUp(ascb_sort_workspace_bytes(nnz, destination_outer), 256);
+  l.total = at;
+  return l;
+}
+
+// The destination of a conversion: caller-allocated device arrays of the
+// other format, validated like any sparse operand (it is canonical once
+// written), disjoint from the source and the workspace.
+Status ValidateDestination(asc_sb_context* ctx, const asc_sb_sparse* d, int element_kind,
+                           std::int64_t rows, std::int64_t columns, std::int64_t nnz,
+                           SparseBytes* bytes) {
+  if (d == nullptr) return Fail(ASC_SB_INVALID_ARGUMENT, "conversion destination cannot be null");
+  if (d->element_kind != element_kind) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "conversion source and destination elements must match");
+  }
+  if (d->rows != rows || d->columns != columns || d->nonzeros != nnz) {
+    return Fail(ASC_SB_SHAPE, "conversion destination shape does not match the source");
+  }
+  asc_sb_sparse trusted = *d;
+  trusted.canonical_structure_trusted = 1;
+  return ascb::host::ValidateSparse(trusted, ctx->device, bytes);
+}
+
+Status ValidateConvertWorkspace(asc_sb_context* ctx, void* workspace, std::size_t bytes,
+                                std::size_t need) {
+  if (bytes < need || (need != 0 && workspace == nullptr)) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "conversion workspace is missing or too small");
+  }
+  if ((reinterpret_cast<std::uintptr_t>(workspace) & 255u) != 0) {
+    return Fail(ASC_SB_MEMORY_ACCESS, "conversion workspace must be 256-byte aligned");
+  }
+  return ascb::host::ValidateDevicePointer(workspace, bytes, ctx->device,
+                                           "CUDA could not inspect conversion workspace");
+}
+
+bool DestinationOverlaps(const asc_sb_sparse& d, const SparseBytes& db, Span other) {
+  return ascb::host::Overlap({d.structure_first, db.first}, other) ||
+         ascb::host::Overlap({d.structure_second, db.second}, other) ||
+         ascb::host::Overlap({d.values, db.values}, other);
+}
+
+}  // namespace
+
+int asc_sb_convert_workspace_size(asc_sb_context* ctx, int64_t rows, int64_t columns,
+                                  int64_t nonzeros, int32_t destination_format, size_t* bytes) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (bytes == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "bytes cannot be null"));
+  if (destination_format != ASC_SB_CSR && destination_format != ASC_SB_CSC) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "conversions produce CSR or CSC"));
+  }
+  if (rows < 0 || columns < 0 || nonzeros < 0) {
+    return Finish(ctx, Fail(ASC_SB_SHAPE, "conversion extents cannot be negative"));
+  }
+  *bytes = ConvertLayoutFor(nonzeros, destination_format == ASC_SB_CSR ? rows : columns).total;
+  return Finish(ctx, Status::Ok());
+}
+
+int asc_sb_convert_compressed(asc_sb_context* ctx, const asc_sb_sparse* source,
+                              const asc_sb_sparse* destination, void* workspace,
+                              size_t workspace_bytes) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  if (source == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "conversion source cannot be null"));
+  }
+  SparseBytes sb, db;
+  s = ascb::host::ValidateSparse(*source, ctx->device, &sb);
+  if (!s.ok()) return Finish(ctx, s);
+  s = ValidateDestination(ctx, destination, source->element_kind, source->rows, source->columns,
+                          source->nonzeros, &db);
+  if (!s.ok()) return Finish(ctx, s);
+  if (destination->format == source->format) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT,
+                            "a compressed conversion goes from CSR to CSC or from CSC to CSR"));
+  }
+  const std::int64_t dest_outer =
+      destination->format == ASC_SB_CSR ? source->rows : source->columns;
+  const ConvertLayout l = ConvertLayoutFor(source->nonzeros, dest_outer);
+  s = ValidateConvertWorkspace(ctx, workspace, workspace_bytes, l.total);
+  if (!s.ok()) return Finish(ctx, s);
+  const Span ws{workspace, workspace_bytes};
+  if (DestinationOverlaps(*destination, db, {source->structure_first, sb.first}) ||
+      DestinationOverlaps(*destination, db, {source->structure_second, sb.second}) ||
+      DestinationOverlaps(*destination, db, {source->values, sb.values}) ||
+      DestinationOverlaps(*destination, db, ws) ||
+      ascb::host::Overlap({source->structure_first, sb.first}, ws) ||
+      ascb::host::Overlap({source->structure_second, sb.second}, ws) ||
+      ascb::host::Overlap({source->values, sb.values}, ws)) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT,
+                            "conversion destination and workspace must not overlap any operand"));
+  }
+  // the source read as CSR arrays: outer = its outer extent, keys = its inner
+  // indices, which become the destination's outer indices
+  const ascb_csr a = AsCsr(*source, source->format == ASC_SB_CSC);
+  auto* w = static_cast<unsigned char*>(workspace);
+  auto* perm = reinterpret_cast<std::int64_t*>(w + l.perm);
+  s = BuildTransposed(ctx, a, ascb::host::ElementBytes(source->element_kind),
+                      static_cast<std::int64_t*>(const_cast<void*>(destination->structure_first)),
+                      static_cast<std::int64_t*>(const_cast<void*>(destination->structure_second)),
+                      perm, const_cast<void*>(destination->values), w + l.sort,
+                      reinterpret_cast<std::int64_t*>(w + l.outer_of));
+  return Finish(ctx, s);
+}
+
+int asc_sb_convert_coordinates(asc_sb_context* ctx, const int64_t* coordinates,
+                               const void* values, int32_t element_kind, int64_t rows,
+                               int64_t columns, int64_t nonzeros,
+                               const asc_sb_sparse* destination, void* workspace,
+                               size_t workspace_bytes) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  if (rows < 0 || columns < 0 || nonzeros < 0) {
+    return Finish(ctx, Fail(ASC_SB_SHAPE, "conversion extents cannot be negative"));
+  }
+  SparseBytes db;
+  s = ValidateDestination(ctx, destination, element_kind, rows, columns, nonzeros, &db);
+  if (!s.ok()) return Finish(ctx, s);
+  const std::size_t element = ascb::host::ElementBytes(element_kind);
+  const Span cs{coordinates, static_cast<std::size_t>(nonzeros) * 16};
+  const Span vs{values, static_cast<std::size_t>(nonzeros) * element};
+  if (nonzeros > 0) {
+    s = ascb::host::ValidateAddress(coordinates, cs.bytes, 8, "coordinate storage is incomplete",
+                                    "coordinate storage is misaligned");
+    if (!s.ok()) return Finish(ctx, s);
+    s = ascb::host::ValidateAddress(values, vs.bytes, element > 8 ? 8 : element,
+                                    "coordinate value storage is incomplete",
+                                    "coordinate value storage is misaligned");
+    if (!s.ok()) return Finish(ctx, s);
+    s = ascb::host::ValidateDevicePointer(coordinates, cs.bytes, ctx->device,
+                                          "CUDA could not inspect coordinate storage");
+    if (!s.ok()) return Finish(ctx, s);
+    s = ascb::host::ValidateDevicePointer(values, vs.bytes, ctx->device,
+                                          "CUDA could not inspect coordinate value storage");
+    if (!s.ok()) return Finish(ctx, s);
+  }
+  const bool to_csr = destination->format == ASC_SB_CSR;
+  const ConvertLayout l = ConvertLayoutFor(nonzeros, to_csr ? rows : columns);
+  s = ValidateConvertWorkspace(ctx, workspace, workspace_bytes, l.total);
+  if (!s.ok()) return Finish(ctx, s);
+  const Span ws{workspace, workspace_bytes};
+  if (DestinationOverlaps(*destination, db, cs) || DestinationOverlaps(*destination, db, vs) ||
+      DestinationOverlaps(*destination, db, ws) || ascb::host::Overlap(cs, ws) ||
+      ascb::host::Overlap(vs, ws)) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT,
+                            "conversion destination and workspace must not overlap any operand"));
+  }
+  auto* w = static_cast<unsigned char*>(workspace);
+  auto* perm = reinterpret_cast<std::int64_t*>(w + l.perm);
+  auto* offsets = static_cast<std::int64_t*>(const_cast<void*>(destination->structure_first));
+  // coordinates are (row, column) pairs: the destination's outer index is the
+  // row for CSR and the column for CSC, the other one becomes the inner index
+  s = Launched(ctx,
+               ascb_stable_sort(ctx->stream, coordinates + (to_csr ? 0 : 1), 2, nonzeros,
+                                to_csr ? rows : columns, offsets, perm, w + l.sort),
+               "CUDA could not launch the conversion sort");
+  if (!s.ok()) return Finish(ctx, s);
+  s = Launched(ctx,
+               ascb_permute_entries(
+                   ctx->stream, perm, nonzeros, coordinates + (to_csr ? 1 : 0), 2,
+                   static_cast<std::int64_t*>(const_cast<void*>(destination->structure_second)),
+                   values, const_cast<void*>(destination->values), static_cast<int>(element),
+                   ctx->sm_count),
+               "CUDA could not launch the entry permutation kernel");
+  return Finish(ctx, s);
 }
 
 }  // extern "C"

@@ -44,6 +44,22 @@ int ascb_merge_path_splits(void* stream, const ascb_csr* a, int64_t items,
                            int64_t* split_row, int64_t* split_nz,
                            int64_t ntiles);
 
+// ---- stable sort by key (format conversions, transposed structure) ----
+// perm[q] = source position of the q-th entry in (key, position) order of
+// keys[e * kstride], e < n; offsets[0..limit] = bucket starts (keys outside
+// [0, limit) are not counted).  `workspace` holds ascb_sort_workspace_bytes.
+size_t ascb_sort_workspace_bytes(int64_t n, int64_t limit);
+int ascb_stable_sort(void* stream, const int64_t* keys, int64_t kstride, int64_t n, int64_t limit,
+                     int64_t* offsets, int64_t* perm, void* workspace);
+// out[q] = r for every entry q in [ptr[r], ptr[r+1]).
+int ascb_outer_of_entries(void* stream, const int64_t* ptr, int64_t outer, int64_t* out,
+                          int sm_count);
+// idx_out[j] = other[perm[j] * ostride] (if idx_out), val_out[j] =
+// val_in[perm[j]] (if val_out; elem_bytes 4, 8 or 16).
+int ascb_permute_entries(void* stream, const int64_t* perm, int64_t n, const int64_t* other,
+                         int64_t ostride, int64_t* idx_out, const void* val_in, void* val_out,
+                         int elem_bytes, int sm_count);
+
 // ---- SpMV variants ----
 // Warp-tiled SpMV over row tiles of ascb_warp_tile_items() weighted items with
 // row weight ascb_warp_tile_row_weight().  exact = 1 reproduces the serial

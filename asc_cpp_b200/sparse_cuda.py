@@ -281,10 +281,16 @@ def CudaSpmv(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
 
 
 def CudaSpmm(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
-             matrix: CudaCsrArray, b: DenseMatrixView, c: DenseMatrixView) -> None:
+             matrix: CudaCsrArray, b: DenseMatrixView, c: DenseMatrixView,
+             plan: "CsrPlan | None" = None) -> None:
     """C += alpha*op(A)*B (blas.h:1692-1750 semantics)."""
     m, bd, cd = matrix.describe(), b.describe(), c.describe()
     bd.writable = 0
+    if plan is not None:
+        context.check(context._lib.asc_sb_plan_standard_spmm(
+            context.handle, plan.handle, int(op), float(alpha), 0.0, ctypes.byref(bd),
+            ctypes.byref(cd)))
+        return
     context.check(context._lib.asc_sb_standard_spmm(
         context.handle, int(op), float(alpha), 0.0, ctypes.byref(m), ctypes.byref(bd),
         ctypes.byref(cd)))
@@ -314,6 +320,11 @@ class CsrPlan:
     def handle(self):
         return self._h
 
+    def refresh_values(self) -> None:
+        """Re-gathers the transposed values after the matrix's values changed."""
+        self.context.check(self.context._lib.asc_sb_plan_refresh_values(
+            self.context.handle, self._h))
+
     def csr_spmv(self, alpha: float, x: CudaStridedVectorView, beta: float,
                  y: CudaStridedVectorView) -> None:
         xd, yd = x.describe(), y.describe()
@@ -332,3 +343,58 @@ class CsrPlan:
             self.close()
         except Exception:
             pass
+
+
+# ---- format conversion on the device (compressed.h:1082-1221 semantics) ----
+
+def _convert_workspace(context: SparseCudaContext, rows: int, columns: int, nnz: int,
+                       fmt: FormatKind) -> torch.Tensor:
+    n = ctypes.c_size_t()
+    context.check(context._lib.asc_sb_convert_workspace_size(
+        context.handle, rows, columns, nnz, int(fmt), ctypes.byref(n)))
+    return torch.empty(max(n.value, 1), dtype=torch.uint8,
+                       device=torch.device("cuda", context.device))
+
+
+def _empty_compressed(context: SparseCudaContext, rows: int, columns: int, nnz: int,
+                      dtype: torch.dtype, fmt: FormatKind) -> CudaCsrArray:
+    dev = torch.device("cuda", context.device)
+    outer = rows if fmt == FormatKind.kCsr else columns
+    return CudaCsrArray(rows, columns, torch.empty(outer + 1, dtype=torch.int64, device=dev),
+                        torch.empty(nnz, dtype=torch.int64, device=dev),
+                        torch.empty(nnz, dtype=dtype, device=dev), fmt)
+
+
+def CudaConvertCompressed(context: SparseCudaContext, source: CudaCsrArray) -> CudaCsrArray:
+    """CSR -> CSC or CSC -> CSR of the same matrix, on the device
+    (ConvertToCsc(CsrView) / ConvertToCsr(CscView), compressed.h:1728-1780)."""
+    fmt = FormatKind.kCsc if source.format == FormatKind.kCsr else FormatKind.kCsr
+    with torch.cuda.stream(context.stream):
+        out = _empty_compressed(context, source.rows, source.columns, source.nnz,
+                                source.values.dtype, fmt)
+        ws = _convert_workspace(context, source.rows, source.columns, source.nnz, fmt)
+    sd, dd = source.describe(), out.describe()
+    dd.canonical_structure_trusted = 0
+    context.check(context._lib.asc_sb_convert_compressed(
+        context.handle, ctypes.byref(sd), ctypes.byref(dd), ws.data_ptr(), ws.numel()))
+    ws.record_stream(context.stream)
+    return out
+
+
+def CudaConvertCoordinates(context: SparseCudaContext, rows: int, columns: int,
+                           coordinates: torch.Tensor, values: torch.Tensor,
+                           fmt: FormatKind = FormatKind.kCsr) -> CudaCsrArray:
+    """Device (row, column) pairs [nnz, 2] + values -> CSR or CSC
+    (ConvertToCsr / ConvertToCsc(CoordinateView), compressed.h:1676-1726)."""
+    nnz = int(values.numel())
+    with torch.cuda.stream(context.stream):
+        out = _empty_compressed(context, rows, columns, nnz, values.dtype, fmt)
+        ws = _convert_workspace(context, rows, columns, nnz, fmt)
+    dd = out.describe()
+    dd.canonical_structure_trusted = 0
+    context.check(context._lib.asc_sb_convert_coordinates(
+        context.handle, coordinates.data_ptr() if nnz else None,
+        values.data_ptr() if nnz else None, _kind(values.dtype), rows, columns, nnz,
+        ctypes.byref(dd), ws.data_ptr(), ws.numel()))
+    ws.record_stream(context.stream)
+    return out

@@ -265,12 +265,60 @@ ASC_SB_API int asc_sb_plan_csr_spmv(asc_sb_context* context,
                                     const asc_sb_plan* plan, double alpha,
                                     const asc_sb_vector* input, double beta,
                                     const asc_sb_vector* output);
-/* Standard SpMV through a plan: same contract as asc_sb_standard_spmv. */
+/* Standard SpMV through a plan: same contract as asc_sb_standard_spmv.  With
+ * ASC_SB_PLAN_TRANSPOSE, a transposed product (op != none on CSR, op = none
+ * on CSC) runs the stored-order kernels on the transposed structure, so it is
+ * available in DETERMINISTIC mode and reproduces the reference's order
+ * (blas.h:1241-1256: outer then inner) bit for bit. */
 ASC_SB_API int asc_sb_plan_standard_spmv(asc_sb_context* context,
                                          const asc_sb_plan* plan, int32_t op,
                                          double alpha_real, double alpha_imag,
                                          const asc_sb_vector* input,
                                          const asc_sb_vector* output);
+/* Standard SpMM through a plan: same contract as asc_sb_standard_spmm, with
+ * the transposed products of asc_sb_plan_standard_spmv. */
+ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
+                                         const asc_sb_plan* plan, int32_t op,
+                                         double alpha_real, double alpha_imag,
+                                         const asc_sb_dense* input,
+                                         const asc_sb_dense* output);
+
+/* ---- format conversion on the device --------------------------------------
+ * Stable conversions of device data, bit-identical to the reference's host
+ * conversions: entries land in the destination grouped by their new outer
+ * index and, within one outer index, in source storage order.  The
+ * destination descriptor names caller-allocated device arrays of the target
+ * format (offsets [outer + 1], indices [nonzeros], values [nonzeros]) with the
+ * source's element kind and shape; they are written on the context stream.
+ * The workspace is device memory, 256-byte aligned, of the queried size; it
+ * may be reused once the stream has passed the call. */
+ASC_SB_API int asc_sb_convert_workspace_size(asc_sb_context* context,
+                                             int64_t rows, int64_t columns,
+                                             int64_t nonzeros,
+                                             int32_t destination_format,
+                                             size_t* bytes);
+/* CSR -> CSC or CSC -> CSR.  Replaces, for device data, asc::ConvertToCsc(
+ * CsrView) and asc::ConvertToCsr(CscView) (include/asc/sparse/compressed.h:
+ * 1728-1780 -> CompressedSparseArray::FromCompressed, :1151-1221). */
+ASC_SB_API int asc_sb_convert_compressed(asc_sb_context* context,
+                                         const asc_sb_sparse* source,
+                                         const asc_sb_sparse* destination,
+                                         void* workspace,
+                                         size_t workspace_bytes);
+/* Coordinates -> CSR or CSC.  `coordinates` holds (row, column) int64 pairs,
+ * [nonzeros][2], the reference's coordinate storage (coordinate.h:267-330);
+ * `values` holds `nonzeros` elements of `element_kind`.  Replaces, for device
+ * data, asc::ConvertToCsr / ConvertToCsc(CoordinateView) (compressed.h:
+ * 1676-1726 -> CompressedSparseArray::FromCoordinate, :1082-1131).  Input in
+ * any order is accepted; canonical input gives canonical output. */
+ASC_SB_API int asc_sb_convert_coordinates(asc_sb_context* context,
+                                          const int64_t* coordinates,
+                                          const void* values,
+                                          int32_t element_kind, int64_t rows,
+                                          int64_t columns, int64_t nonzeros,
+                                          const asc_sb_sparse* destination,
+                                          void* workspace,
+                                          size_t workspace_bytes);
 
 #ifdef __cplusplus
 }  /* extern "C" */

@@ -77,6 +77,9 @@ class Restatement:
         self.lib.oracle_csr_transpose_structure.restype = None
         self.lib.oracle_csr_transpose_structure.argtypes = [_I64, _I64, _P, _P,
                                                             _P, _P, _P]
+        self.lib.oracle_stable_bucket_sort.restype = None
+        self.lib.oracle_stable_bucket_sort.argtypes = [_I64, _P, _I64, _I64,
+                                                       _P, _P]
         self.lib.oracle_merge_path_split.restype = None
         self.lib.oracle_merge_path_split.argtypes = [
             _I64, _P, _I64, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_I64)]
@@ -136,6 +139,35 @@ class Restatement:
                                                 _ptr(t_idx), _ptr(perm))
         return t_ptr, t_idx[:nnz], perm[:nnz]
 
+    def stable_bucket_sort(self, keys, kstride, n, limit):
+        """(offsets[limit+1], perm[n]) of the stable sort of keys[e*kstride]."""
+        offsets = np.zeros(limit + 1, dtype=np.int64)
+        perm = np.zeros(max(n, 1), dtype=np.int64)
+        keys = np.ascontiguousarray(keys, dtype=np.int64)
+        self.lib.oracle_stable_bucket_sort(n, _ptr(keys), kstride, limit,
+                                           _ptr(offsets), _ptr(perm))
+        return offsets, perm[:n]
+
+    def convert_compressed(self, to_csc, rows, cols, ptr, idx, val):
+        """CSR arrays -> CSC arrays (to_csc) or CSC -> CSR, stable order."""
+        outer_in = rows if to_csc else cols
+        outer_out = cols if to_csc else rows
+        nnz = int(ptr[outer_in])
+        offsets, perm = self.stable_bucket_sort(idx, 1, nnz, outer_out)
+        source_outer = np.repeat(np.arange(outer_in, dtype=np.int64),
+                                 np.diff(ptr))
+        return offsets, source_outer[perm], val[perm]
+
+    def convert_coordinates(self, to_csc, rows, cols, coordinates, val):
+        """Interleaved [nnz][2] coordinates -> CSR (to_csc = 0) or CSC."""
+        nnz = len(val)
+        c = np.ascontiguousarray(coordinates, dtype=np.int64).reshape(-1)
+        key = c[1:] if to_csc else c
+        other = c[0::2] if to_csc else c[1::2]
+        offsets, perm = self.stable_bucket_sort(key, 2, nnz,
+                                                cols if to_csc else rows)
+        return offsets, other[perm], val[perm]
+
     def merge_path_split(self, ptr, diagonal):
         rows = len(ptr) - 1
         r = _I64()
@@ -176,6 +208,12 @@ class Reference:
             f = getattr(self.lib, f"ref_blocks_free_{sfx}")
             f.restype = None
             f.argtypes = [_P]
+        f = self.lib.ref_convert_compressed_f64
+        f.restype = _INT
+        f.argtypes = [_INT, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P]
+        f = self.lib.ref_convert_coordinates_f64
+        f.restype = _INT
+        f.argtypes = [_INT, _I64, _I64, _P, _P, _I64, _P, _P, _P]
 
     @staticmethod
     def available() -> bool:
@@ -227,3 +265,32 @@ class Reference:
 
     def blocks_free(self, h, dtype) -> None:
         getattr(self.lib, f"ref_blocks_free_{_suffix(dtype)}")(h)
+
+    # conversions (FP64 values), the reference's ConvertToCsr / ConvertToCsc
+    def convert_compressed(self, to_csc, rows, cols, ptr, idx, val):
+        outer_in = rows if to_csc else cols
+        outer_out = cols if to_csc else rows
+        nnz = int(ptr[outer_in])
+        o = np.zeros(outer_out + 1, dtype=np.int64)
+        i = np.zeros(max(nnz, 1), dtype=np.int64)
+        v = np.zeros(max(nnz, 1), dtype=np.float64)
+        rc = self.lib.ref_convert_compressed_f64(
+            int(to_csc), rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), nnz,
+            _ptr(o), _ptr(i), _ptr(v))
+        if rc != 0:
+            raise RuntimeError(f"reference conversion failed with code {rc}")
+        return o, i[:nnz], v[:nnz]
+
+    def convert_coordinates(self, to_csc, rows, cols, coordinates, val):
+        nnz = len(val)
+        c = np.ascontiguousarray(coordinates, dtype=np.int64).reshape(-1)
+        outer_out = cols if to_csc else rows
+        o = np.zeros(outer_out + 1, dtype=np.int64)
+        i = np.zeros(max(nnz, 1), dtype=np.int64)
+        v = np.zeros(max(nnz, 1), dtype=np.float64)
+        rc = self.lib.ref_convert_coordinates_f64(
+            int(to_csc), rows, cols, _ptr(c), _ptr(val), nnz, _ptr(o), _ptr(i),
+            _ptr(v))
+        if rc != 0:
+            raise RuntimeError(f"reference conversion failed with code {rc}")
+        return o, i[:nnz], v[:nnz]

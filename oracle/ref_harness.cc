@@ -13,6 +13,9 @@
 //                   include/asc/sparse/blas.h:1607-1667
 //   * standard SpMM asc::Spmm(ctx, op, alpha, CompressedSparseView, B, C)
 //                   include/asc/sparse/blas.h:1692-1750
+//   * conversions   asc::ConvertToCsr / ConvertToCsc (compressed.h:1676-1780)
+//                   -> CompressedSparseArray::FromCompressed (:1151-1221)
+//                   and FromCoordinate (:1082-1131)
 // Return value: the reference's asc::ErrorCode as an int (0 == kOk).
 
 #include <algorithm>
@@ -32,6 +35,7 @@
 #include "asc/expression/writable.h"
 #include "asc/sparse/blas.h"
 #include "asc/sparse/compressed.h"
+#include "asc/sparse/coordinate.h"
 
 // A strided host vector made visible to the reference's expression protocol.
 template <typename T>
@@ -260,6 +264,68 @@ int RunBlocks(void* handle, T alpha, const T* x, T beta, T* y) {
   return 0;
 }
 
+// Copies a reference-owned compressed array out to caller buffers
+// (outer offsets [outer+1], inner indices [nnz], values [nnz]).
+template <typename Array, typename T>
+int CopyOut(Array& array, std::int64_t outer, std::int64_t* out_ptr,
+            std::int64_t* out_idx, T* out_val) {
+  auto view = array.view();
+  if (!view.ok()) return Code(view.status());
+  const std::int64_t nnz = view->nnz();
+  std::copy(view->outer_offsets(), view->outer_offsets() + outer + 1, out_ptr);
+  std::copy(view->inner_indices(), view->inner_indices() + nnz, out_idx);
+  std::copy(view->values(), view->values() + nnz, out_val);
+  return 0;
+}
+
+// to_csc = 1: CSR arrays in, CSC arrays out; 0: CSC in, CSR out.
+template <typename T>
+int ConvertCompressed(int to_csc, std::int64_t rows, std::int64_t cols,
+                      const std::int64_t* ptr, const std::int64_t* idx,
+                      const T* val, std::int64_t nnz, std::int64_t* out_ptr,
+                      std::int64_t* out_idx, T* out_val) {
+  const std::array<asc::extent_t, 2> shape{rows, cols};
+  asc::HostMemoryResource resource;
+  const auto context = asc::ExecutionContext::Serial();
+  if (to_csc) {
+    auto src = asc::CsrView<const T>::Create(ptr, idx, val, shape, nnz,
+                                             asc::MemorySpace::kHost);
+    if (!src.ok()) return Code(src.status());
+    auto dst = asc::ConvertToCsc<const T>(context, *src, resource);
+    if (!dst.ok()) return Code(dst.status());
+    return CopyOut(*dst, cols, out_ptr, out_idx, out_val);
+  }
+  auto src = asc::CscView<const T>::Create(ptr, idx, val, shape, nnz,
+                                           asc::MemorySpace::kHost);
+  if (!src.ok()) return Code(src.status());
+  auto dst = asc::ConvertToCsr<const T>(context, *src, resource);
+  if (!dst.ok()) return Code(dst.status());
+  return CopyOut(*dst, rows, out_ptr, out_idx, out_val);
+}
+
+// Canonical coordinates (interleaved [nnz][2]) to CSR (to_csc = 0) or CSC.
+template <typename T>
+int ConvertCoordinates(int to_csc, std::int64_t rows, std::int64_t cols,
+                       const std::int64_t* coordinates, const T* val,
+                       std::int64_t nnz, std::int64_t* out_ptr,
+                       std::int64_t* out_idx, T* out_val) {
+  const std::array<asc::extent_t, 2> shape{rows, cols};
+  asc::HostMemoryResource resource;
+  const auto context = asc::ExecutionContext::Serial();
+  auto src = asc::CoordinateView<const T, 2>::Create(
+      coordinates, val, std::span<const asc::extent_t, 2>(shape), nnz,
+      asc::MemorySpace::kHost);
+  if (!src.ok()) return Code(src.status());
+  if (to_csc) {
+    auto dst = asc::ConvertToCsc<const T>(context, *src, resource);
+    if (!dst.ok()) return Code(dst.status());
+    return CopyOut(*dst, cols, out_ptr, out_idx, out_val);
+  }
+  auto dst = asc::ConvertToCsr<const T>(context, *src, resource);
+  if (!dst.ok()) return Code(dst.status());
+  return CopyOut(*dst, rows, out_ptr, out_idx, out_val);
+}
+
 }  // namespace
 
 extern "C" {
@@ -342,5 +408,23 @@ int ref_blocks_run_f32(void* h, float alpha, const float* x, float beta,
 }
 void ref_blocks_free_f64(void* h) { delete static_cast<Blocks<double>*>(h); }
 void ref_blocks_free_f32(void* h) { delete static_cast<Blocks<float>*>(h); }
+
+int ref_convert_compressed_f64(int to_csc, std::int64_t rows,
+                               std::int64_t cols, const std::int64_t* ptr,
+                               const std::int64_t* idx, const double* val,
+                               std::int64_t nnz, std::int64_t* out_ptr,
+                               std::int64_t* out_idx, double* out_val) {
+  return ConvertCompressed<double>(to_csc, rows, cols, ptr, idx, val, nnz,
+                                   out_ptr, out_idx, out_val);
+}
+int ref_convert_coordinates_f64(int to_csc, std::int64_t rows,
+                                std::int64_t cols,
+                                const std::int64_t* coordinates,
+                                const double* val, std::int64_t nnz,
+                                std::int64_t* out_ptr, std::int64_t* out_idx,
+                                double* out_val) {
+  return ConvertCoordinates<double>(to_csc, rows, cols, coordinates, val, nnz,
+                                    out_ptr, out_idx, out_val);
+}
 
 }  // extern "C"

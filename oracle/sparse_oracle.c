@@ -197,6 +197,36 @@ void oracle_csr_transpose_structure(int64_t rows, int64_t cols,
 }
 
 /* ------------------------------------------------------------------------- */
+/* Stable bucket sort of n entries by key = keys[e * kstride] in [0, limit):
+ * offsets[0..limit] are the bucket starts, perm[q] the source position of the
+ * q-th entry in (key, source position) order.  It is the order in which the
+ * reference's conversions emit entries: FromCompressed scans every source
+ * outer in order for each destination outer (compressed.h:1151-1221) and
+ * FromCoordinate scans every coordinate in stored order for each destination
+ * outer (compressed.h:1082-1131), so within one destination outer entries
+ * keep their source order.  Keys outside [0, limit) are a contract violation
+ * and are left out (their perm slots are -1 at the end). */
+void oracle_stable_bucket_sort(int64_t n, const int64_t* keys, int64_t kstride,
+                               int64_t limit, int64_t* offsets,
+                               int64_t* perm) {
+  memset(offsets, 0, (size_t)(limit + 1) * sizeof(int64_t));
+  for (int64_t e = 0; e < n; ++e) {
+    const int64_t k = keys[e * kstride];
+    if (k >= 0 && k < limit) offsets[k + 1] += 1;
+  }
+  for (int64_t k = 0; k < limit; ++k) offsets[k + 1] += offsets[k];
+  int64_t* next = (int64_t*)malloc((size_t)(limit > 0 ? limit : 1) * sizeof(int64_t));
+  if (next == NULL) return;
+  memcpy(next, offsets, (size_t)limit * sizeof(int64_t));
+  for (int64_t q = offsets[limit]; q < n; ++q) perm[q] = -1;
+  for (int64_t e = 0; e < n; ++e) {
+    const int64_t k = keys[e * kstride];
+    if (k >= 0 && k < limit) perm[next[k]++] = e;
+  }
+  free(next);
+}
+
+/* ------------------------------------------------------------------------- */
 /* Merge-path split of the (row-end, nonzero) merge of a CSR matrix.
  * The merge interleaves list A = ptr[1..rows] (the end offset of each row)
  * with list B = 0, 1, ..., nnz-1 (the nonzero positions), taking a nonzero

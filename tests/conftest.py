@@ -37,6 +37,11 @@ def known_answers():
 
 
 @pytest.fixture(scope="session")
+def conversions():
+    return dict(np.load(os.path.join(GOLDEN, "conversions.npz")))
+
+
+@pytest.fixture(scope="session")
 def random_cases():
     return dict(np.load(os.path.join(GOLDEN, "random_cases.npz")))
 

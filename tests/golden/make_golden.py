@@ -23,6 +23,10 @@ into oracle/_ref/libasc_ref.so by oracle/build_oracle.py).  The fixtures pin:
 * ``laplacian.npz`` - the 5-point Laplacian on a 316 x 316 grid
   (alpha = 1, beta = 0.5, x and y uniform[-1, 1] from seed 0): SHA-256 of the
   reference's output bytes and a strided sample of the output.
+* ``conversions.npz`` - the reference's CSR -> CSC, CSC -> CSR and
+  coordinate -> CSR / CSC conversions (compressed.h:1676-1780) of the
+  conversion test's 3 x 4 matrix (tests/sparse/compressed_conversion_test.cc:
+  28-36) and of seeded random matrices with empty rows and columns.
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -177,13 +181,48 @@ def laplacian(ref: Reference) -> dict[str, np.ndarray]:
             "sample": y[::997].copy()}
 
 
+def conversions(ref: Reference) -> dict[str, np.ndarray]:
+    """Reference conversions (ConvertToCsc / ConvertToCsr, compressed.h:
+    1676-1780) of the conversion test's 3x4 matrix (compressed_conversion_
+    test.cc:28-36) and of seeded random matrices with empty rows and columns."""
+    out: dict[str, np.ndarray] = {}
+    ptr = np.array([0, 2, 4, 5], np.int64)
+    idx = np.array([1, 3, 0, 2, 1], np.int64)
+    val = np.array([2.0, -1.0, 4.0, 5.0, 3.0])
+    coords = np.array([0, 1, 0, 3, 1, 0, 1, 2, 2, 1], np.int64)
+    cases = {"ka": (3, 4, ptr, idx, val, coords)}
+    rng = np.random.default_rng(21)
+    for name, (r, c, m) in {"r1": (60, 45, 12), "r2": (1, 300, 40), "r3": (300, 1, 1),
+                            "r4": (200, 700, 9)}.items():
+        a = synthetic.random_csr(rng, r, c, m, np.float64, 0.2)
+        rows_of = np.repeat(np.arange(r, dtype=np.int64), np.diff(a.ptr))
+        co = np.stack([rows_of, a.idx], axis=1).reshape(-1)
+        cases[name] = (r, c, a.ptr, a.idx, a.val, co)
+    for name, (r, c, p_, i_, v_, co) in cases.items():
+        out[f"{name}_shape"] = np.array([r, c], np.int64)
+        out[f"{name}_csr_ptr"], out[f"{name}_csr_idx"], out[f"{name}_csr_val"] = p_, i_, v_
+        out[f"{name}_coo"] = co
+        o, i, v = ref.convert_compressed(1, r, c, p_, i_, v_)
+        out[f"{name}_csc_ptr"], out[f"{name}_csc_idx"], out[f"{name}_csc_val"] = o, i, v
+        back = ref.convert_compressed(0, r, c, o, i, v)
+        for k, arr in zip(("ptr", "idx", "val"), back):
+            out[f"{name}_csc_to_csr_{k}"] = arr
+        for fmt, to_csc in (("csr", 0), ("csc", 1)):
+            o2, i2, v2 = ref.convert_coordinates(to_csc, r, c, co, v_)
+            out[f"{name}_coo_to_{fmt}_ptr"] = o2
+            out[f"{name}_coo_to_{fmt}_idx"] = i2
+            out[f"{name}_coo_to_{fmt}_val"] = v2
+    return out
+
+
 def main() -> None:
     build_oracle.build_reference()
     ref = Reference()
     np.savez_compressed(os.path.join(HERE, "known_answers.npz"), **known_answers(ref))
     np.savez_compressed(os.path.join(HERE, "random_cases.npz"), **random_cases(ref))
     np.savez_compressed(os.path.join(HERE, "laplacian.npz"), **laplacian(ref))
-    for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz"):
+    np.savez_compressed(os.path.join(HERE, "conversions.npz"), **conversions(ref))
+    for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz", "conversions.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))
 
 

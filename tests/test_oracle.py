@@ -173,3 +173,45 @@ def test_merge_path_split_properties(restatement):
         if r < a.rows:
             assert a.ptr[r + 1] >= z
         prev = (r, z)
+
+
+CONVERSION_CASES = ("ka", "r1", "r2", "r3", "r4")
+
+
+@pytest.mark.parametrize("name", CONVERSION_CASES)
+def test_conversions_match_reference_fixtures(restatement, conversions, name):
+    """The oracle's stable bucket sort reproduces the reference's conversions
+    (compressed.h:1082-1221) on the committed fixtures."""
+    g = conversions
+    r, c = (int(v) for v in g[f"{name}_shape"])
+    ptr, idx, val = g[f"{name}_csr_ptr"], g[f"{name}_csr_idx"], g[f"{name}_csr_val"]
+    got = restatement.convert_compressed(1, r, c, ptr, idx, val)
+    for k, arr in zip(("ptr", "idx", "val"), got):
+        assert _bits_equal(arr, g[f"{name}_csc_{k}"])
+    back = restatement.convert_compressed(0, r, c, g[f"{name}_csc_ptr"], g[f"{name}_csc_idx"],
+                                          g[f"{name}_csc_val"])
+    for k, arr in zip(("ptr", "idx", "val"), back):
+        assert _bits_equal(arr, g[f"{name}_csc_to_csr_{k}"])
+        assert _bits_equal(arr, g[f"{name}_csr_{k}"])
+    for fmt, to_csc in (("csr", 0), ("csc", 1)):
+        got = restatement.convert_coordinates(to_csc, r, c, g[f"{name}_coo"], val)
+        for k, arr in zip(("ptr", "idx", "val"), got):
+            assert _bits_equal(arr, g[f"{name}_coo_to_{fmt}_{k}"])
+
+
+def test_conversion_known_answer_values(conversions):
+    """compressed_conversion_test.cc:28-36 expected CSC arrays."""
+    assert conversions["ka_csc_ptr"].tolist() == [0, 1, 3, 4, 5]
+    assert conversions["ka_csc_idx"].tolist() == [1, 0, 2, 1, 0]
+    assert conversions["ka_csc_val"].tolist() == [4.0, 2.0, 3.0, 5.0, -1.0]
+
+
+def test_conversion_matches_reference_directly(restatement, reference):
+    from asc_cpp_b200 import synthetic
+    rng = np.random.default_rng(22)
+    a = synthetic.random_csr(rng, 150, 90, 20, np.float64, 0.3)
+    for to_csc in (1,):
+        got = restatement.convert_compressed(to_csc, a.rows, a.cols, a.ptr, a.idx, a.val)
+        want = reference.convert_compressed(to_csc, a.rows, a.cols, a.ptr, a.idx, a.val)
+        for x, y in zip(got, want):
+            assert _bits_equal(x, y)
