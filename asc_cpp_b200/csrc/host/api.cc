@@ -100,9 +100,22 @@ Status Launched(asc_sb_context* ctx, int err, const char* message) {
           std::string(message) + ": " + cudaGetErrorString(static_cast<cudaError_t>(err))};
 }
 
-int Dtype(int kind) { return kind == ASC_SB_DOUBLE ? ASCB_F64 : ASCB_F32; }
-
 bool RealKind(int kind) { return kind == ASC_SB_FLOAT || kind == ASC_SB_DOUBLE; }
+
+int Dtype(int kind) {
+  switch (kind) {
+    case ASC_SB_DOUBLE: return ASCB_F64;
+    case ASC_SB_COMPLEX_FLOAT: return ASCB_C64;
+    case ASC_SB_COMPLEX_DOUBLE: return ASCB_C128;
+    default: return ASCB_F32;
+  }
+}
+
+// alpha == 0 in the element type: real kinds take the real part only, as the
+// reference's ScalarValue conversion does (kernels.cu:15-17, 45-47).
+bool AlphaIsZero(int kind, double alpha_real, double alpha_imag) {
+  return RealKind(kind) ? alpha_real == 0.0 : (alpha_real == 0.0 && alpha_imag == 0.0);
+}
 
 ascb_csr AsCsr(const asc_sb_sparse& m, bool swap_shape) {
   ascb_csr a{};
@@ -555,8 +568,7 @@ struct StandardOperands {
   Span in_span, out_span;
 };
 
-Status ValidateStandardSpmv(asc_sb_context* ctx, int op, double alpha_imag,
-                            const asc_sb_sparse* m, const asc_sb_vector* x,
+Status ValidateStandardSpmv(asc_sb_context* ctx, int op, const asc_sb_sparse* m, const asc_sb_vector* x,
                             const asc_sb_vector* y, StandardOperands* out) {
   if (op != ASC_SB_OP_NONE && op != ASC_SB_OP_TRANSPOSE && op != ASC_SB_OP_CONJUGATE_TRANSPOSE) {
     return Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS transpose mode is invalid");
@@ -566,9 +578,6 @@ Status ValidateStandardSpmv(asc_sb_context* ctx, int op, double alpha_imag,
   }
   Status s = ascb::host::ValidateSparse(*m, ctx->device, &out->matrix_bytes);
   if (!s.ok()) return s;
-  if (!RealKind(m->element_kind) || alpha_imag != 0.0) {
-    return Fail(ASC_SB_UNSUPPORTED, "CUDA standardized SpMV supports real float and double");
-  }
   s = ascb::host::ValidateVector(*x, m->element_kind, false, ctx->device, &out->in_span);
   if (!s.ok()) return s;
   s = ascb::host::ValidateVector(*y, m->element_kind, true, ctx->device, &out->out_span);
@@ -605,13 +614,29 @@ ascb_csr TransposedCsr(const asc_sb_plan& plan) {
 // (for CSC: the CSR of A^T); `transposed` says whether the product needs the
 // transpose of those arrays.
 Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
-                       const asc_sb_sparse& m, int op, double alpha,
+                       const asc_sb_sparse& m, int op, double alpha, double alpha_imag,
                        const asc_sb_vector& x, const asc_sb_vector& y) {
   const bool csc = m.format == ASC_SB_CSC;
   const bool transposed = (op != ASC_SB_OP_NONE) != csc;
   const ascb_csr a = AsCsr(m, csc);
   const int dtype = Dtype(m.element_kind);
   const ascb_vec xv = AsVec(x), yv = AsVec(y);
+  if (!RealKind(m.element_kind)) {
+    const bool planned = transposed && plan != nullptr && plan->t_ptr != nullptr;
+    const bool exact = ctx->determinism == ASC_SB_DETERMINISTIC;
+    if (transposed && !planned && exact) {
+      return Fail(ASC_SB_INVALID_STATE,
+                  "A deterministic transposed product needs a plan created with "
+                  "ASC_SB_PLAN_TRANSPOSE");
+    }
+    const ascb_csr rows_of_op = planned ? TransposedCsr(*plan) : a;
+    const int mode = transposed && !planned ? 2 : (exact ? 1 : 0);
+    return Launched(ctx,
+                    ascb_complex_spmv(ctx->stream, dtype, mode,
+                                      op == ASC_SB_OP_CONJUGATE_TRANSPOSE ? 1 : 0, &rows_of_op,
+                                      alpha, alpha_imag, &xv, &yv, ctx->sm_count),
+                    "CUDA could not launch the complex SpMV kernel");
+  }
   if (!transposed) {
     const Choice choice = Choose(ctx, m);
     return RunCsr(ctx, choice, ASCB_STANDARD, a, dtype, alpha, 0.0, xv, yv, nullptr,
@@ -642,10 +667,12 @@ int asc_sb_standard_spmv(asc_sb_context* ctx, int32_t op, double alpha_real, dou
   DeviceGuard guard(ctx->device);
   if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
   StandardOperands ops;
-  s = ValidateStandardSpmv(ctx, op, alpha_imag, m, x, y, &ops);
+  s = ValidateStandardSpmv(ctx, op, m, x, y, &ops);
   if (!s.ok()) return Finish(ctx, s);
-  if (alpha_real == 0.0 || y->extent == 0) return Finish(ctx, Status::Ok());
-  return Finish(ctx, RunStandardSpmv(ctx, nullptr, *m, op, alpha_real, *x, *y));
+  if (AlphaIsZero(m->element_kind, alpha_real, alpha_imag) || y->extent == 0) {
+    return Finish(ctx, Status::Ok());
+  }
+  return Finish(ctx, RunStandardSpmv(ctx, nullptr, *m, op, alpha_real, alpha_imag, *x, *y));
 }
 
 // ---------------------------------------------------------------------------
@@ -666,9 +693,6 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
   SparseBytes mb;
   Status s = ascb::host::ValidateSparse(*m, ctx->device, &mb);
   if (!s.ok()) return s;
-  if (!RealKind(m->element_kind) || alpha_imag != 0.0) {
-    return Fail(ASC_SB_UNSUPPORTED, "CUDA standardized SpMM supports real float and double");
-  }
   Span bs, cs;
   s = ascb::host::ValidateDense(*b, m->element_kind, false, ctx->device, &bs);
   if (!s.ok()) return s;
@@ -684,7 +708,9 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
       ascb::host::Overlap({m->values, mb.values}, cs)) {
     return Fail(ASC_SB_INVALID_ARGUMENT, "CUDA standardized SpMM output overlaps an input");
   }
-  if (alpha_real == 0.0 || c->rows == 0 || c->columns == 0) return Status::Ok();
+  if (AlphaIsZero(m->element_kind, alpha_real, alpha_imag) || c->rows == 0 || c->columns == 0) {
+    return Status::Ok();
+  }
   const bool csc = m->format == ASC_SB_CSC;
   const bool transposed = (op != ASC_SB_OP_NONE) != csc;
   const bool planned = transposed && plan != nullptr && plan->t_ptr != nullptr;
@@ -694,6 +720,17 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
                 "ASC_SB_PLAN_TRANSPOSE");
   }
   const ascb_csr a = planned ? TransposedCsr(*plan) : AsCsr(*m, csc);
+  if (!RealKind(m->element_kind)) {
+    const int mode = transposed && !planned ? 2 : (ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0);
+    return Launched(ctx,
+                    ascb_complex_spmm(ctx->stream, Dtype(m->element_kind), mode,
+                                      op == ASC_SB_OP_CONJUGATE_TRANSPOSE ? 1 : 0, &a, c->columns,
+                                      b->data, b->layout, b->leading_dimension,
+                                      const_cast<void*>(c->data), c->layout,
+                                      c->leading_dimension, alpha_real, alpha_imag,
+                                      ctx->sm_count),
+                    "CUDA could not launch the complex SpMM kernel");
+  }
   return Launched(ctx,
                   ascb_spmm(ctx->stream, Dtype(m->element_kind), transposed && !planned ? 1 : 0,
                             &a, c->columns, b->data, b->layout, b->leading_dimension,
@@ -830,10 +867,13 @@ int asc_sb_plan_standard_spmv(asc_sb_context* ctx, const asc_sb_plan* plan, int3
   std::lock_guard<std::mutex> lock(ctx->mutex);
   DeviceGuard guard(ctx->device);
   StandardOperands ops;
-  s = ValidateStandardSpmv(ctx, op, alpha_imag, &plan->matrix, x, y, &ops);
+  s = ValidateStandardSpmv(ctx, op, &plan->matrix, x, y, &ops);
   if (!s.ok()) return Finish(ctx, s);
-  if (alpha_real == 0.0 || y->extent == 0) return Finish(ctx, Status::Ok());
-  return Finish(ctx, RunStandardSpmv(ctx, plan, plan->matrix, op, alpha_real, *x, *y));
+  if (AlphaIsZero(plan->matrix.element_kind, alpha_real, alpha_imag) || y->extent == 0) {
+    return Finish(ctx, Status::Ok());
+  }
+  return Finish(ctx,
+                RunStandardSpmv(ctx, plan, plan->matrix, op, alpha_real, alpha_imag, *x, *y));
 }
 
 int asc_sb_plan_standard_spmm(asc_sb_context* ctx, const asc_sb_plan* plan, int32_t op,

@@ -26,7 +26,8 @@ typedef struct ascb_vec {
   int64_t stride;  // may be negative
 } ascb_vec;
 
-enum { ASCB_F32 = 0, ASCB_F64 = 1 };
+// complex kinds hold (re, im) pairs, the layout of std::complex
+enum { ASCB_F32 = 0, ASCB_F64 = 1, ASCB_C64 = 2, ASCB_C128 = 3 };
 enum { ASCB_COL_MAJOR = 0, ASCB_ROW_MAJOR = 1 };
 // Arithmetic forms: COMPAT is y = alpha*(sum v x) + beta*y (reference_blas.cc);
 // STANDARD is y += (alpha*v)*x per entry (blas.h:1653-1665).
@@ -92,6 +93,17 @@ int ascb_spmv_vector(void* stream, int dtype, int form, int lanes,
 // Transposed SpMV by scatter: y[c] += alpha * v * x[r] with atomics.
 int ascb_spmv_scatter(void* stream, int dtype, const ascb_csr* a, double alpha,
                       const ascb_vec* x, const ascb_vec* y, int sm_count);
+
+// ---- complex standard products (dtype ASCB_C64 / ASCB_C128) ----
+// mode 0: rows of `a`, any summation order; 1: rows of `a`, the reference's
+// order and rounding; 2: scatter of the transpose of `a` (atomics).  conj = 1
+// conjugates the stored values.
+int ascb_complex_spmv(void* stream, int dtype, int mode, int conj, const ascb_csr* a,
+                      double alpha_re, double alpha_im, const ascb_vec* x, const ascb_vec* y,
+                      int sm_count);
+int ascb_complex_spmm(void* stream, int dtype, int mode, int conj, const ascb_csr* a, int64_t k,
+                      const void* b, int b_layout, int64_t ldb, void* c, int c_layout,
+                      int64_t ldc, double alpha_re, double alpha_im, int sm_count);
 
 // ---- SpMM: C += alpha * op(A) * B (k right-hand sides) ----
 // transpose = 0: bit-exact stored-order kernel; 1: atomic scatter.

@@ -43,6 +43,10 @@ def _kind(dtype: torch.dtype) -> int:
         return ElementKind.kDouble
     if dtype == torch.float32:
         return ElementKind.kFloat
+    if dtype == torch.complex64:
+        return ElementKind.kComplexFloat
+    if dtype == torch.complex128:
+        return ElementKind.kComplexDouble
     raise TypeError(f"unsupported element type {dtype}")
 
 
@@ -270,13 +274,14 @@ def CudaSpmv(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
     """y += alpha*op(A)*x (blas.h:1607-1667 semantics)."""
     m, xd, yd = matrix.describe(), x.describe(), y.describe()
     xd.writable = 0
+    a = complex(alpha)
     if plan is not None:
         context.check(context._lib.asc_sb_plan_standard_spmv(
-            context.handle, plan.handle, int(op), float(alpha), 0.0, ctypes.byref(xd),
+            context.handle, plan.handle, int(op), a.real, a.imag, ctypes.byref(xd),
             ctypes.byref(yd)))
         return
     context.check(context._lib.asc_sb_standard_spmv(
-        context.handle, int(op), float(alpha), 0.0, ctypes.byref(m), ctypes.byref(xd),
+        context.handle, int(op), a.real, a.imag, ctypes.byref(m), ctypes.byref(xd),
         ctypes.byref(yd)))
 
 
@@ -286,13 +291,14 @@ def CudaSpmm(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
     """C += alpha*op(A)*B (blas.h:1692-1750 semantics)."""
     m, bd, cd = matrix.describe(), b.describe(), c.describe()
     bd.writable = 0
+    a = complex(alpha)
     if plan is not None:
         context.check(context._lib.asc_sb_plan_standard_spmm(
-            context.handle, plan.handle, int(op), float(alpha), 0.0, ctypes.byref(bd),
+            context.handle, plan.handle, int(op), a.real, a.imag, ctypes.byref(bd),
             ctypes.byref(cd)))
         return
     context.check(context._lib.asc_sb_standard_spmm(
-        context.handle, int(op), float(alpha), 0.0, ctypes.byref(m), ctypes.byref(bd),
+        context.handle, int(op), a.real, a.imag, ctypes.byref(m), ctypes.byref(bd),
         ctypes.byref(cd)))
 
 

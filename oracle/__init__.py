@@ -40,6 +40,19 @@ def _scalar(dtype):
     return ctypes.c_double if np.dtype(dtype) == np.float64 else ctypes.c_float
 
 
+def _complex_suffix(dtype) -> str | None:
+    dt = np.dtype(dtype)
+    if dt == np.complex128:
+        return "z"
+    if dt == np.complex64:
+        return "c"
+    return None
+
+
+def _real_scalar(dtype):
+    return ctypes.c_double if np.dtype(dtype) == np.complex128 else ctypes.c_float
+
+
 def _suffix(dtype) -> str:
     dt = np.dtype(dtype)
     if dt == np.float64:
@@ -72,6 +85,15 @@ class Restatement:
             f = getattr(self.lib, f"oracle_csr_extended_{sfx}")
             f.restype = None
             f.argtypes = [_INT, _I64, _I64, _P, _P, _P, _P, _P, _P]
+        for sfx, sc in (("z", ctypes.c_double), ("c", ctypes.c_float)):
+            f = getattr(self.lib, f"oracle_complex_spmv_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, sc, sc, _P, _I64,
+                          _P, _I64]
+            f = getattr(self.lib, f"oracle_complex_spmm_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, sc, sc, _P, _INT,
+                          _I64, _P, _INT, _I64, _I64]
         self.lib.oracle_output_counts.restype = None
         self.lib.oracle_output_counts.argtypes = [_INT, _I64, _I64, _P, _P, _P]
         self.lib.oracle_csr_transpose_structure.restype = None
@@ -96,9 +118,17 @@ class Restatement:
     def standard_spmv(self, fmt, op, rows, cols, ptr, idx, val, alpha, x, y,
                       incx=1, incy=1, x_offset=0, y_offset=0):
         """y += alpha*op(A)*x; ``*_offset`` = element index of logical 0."""
-        sc = _scalar(val.dtype)
         xs = x.ctypes.data + x_offset * x.itemsize
         ys = y.ctypes.data + y_offset * y.itemsize
+        cs = _complex_suffix(val.dtype)
+        if cs is not None:
+            rs = _real_scalar(val.dtype)
+            a = complex(alpha)
+            getattr(self.lib, f"oracle_complex_spmv_{cs}")(
+                fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), rs(a.real),
+                rs(a.imag), xs, incx, ys, incy)
+            return y
+        sc = _scalar(val.dtype)
         getattr(self.lib, f"oracle_standard_spmv_{_suffix(val.dtype)}")(
             fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), sc(alpha), xs,
             incx, ys, incy)
@@ -106,6 +136,14 @@ class Restatement:
 
     def standard_spmm(self, fmt, op, rows, cols, ptr, idx, val, alpha, b,
                       b_layout, ldb, c, c_layout, ldc, ncols):
+        cs = _complex_suffix(val.dtype)
+        if cs is not None:
+            rs = _real_scalar(val.dtype)
+            a = complex(alpha)
+            getattr(self.lib, f"oracle_complex_spmm_{cs}")(
+                fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), rs(a.real),
+                rs(a.imag), _ptr(b), b_layout, ldb, _ptr(c), c_layout, ldc, ncols)
+            return c
         sc = _scalar(val.dtype)
         getattr(self.lib, f"oracle_standard_spmm_{_suffix(val.dtype)}")(
             fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val), sc(alpha),
@@ -208,6 +246,16 @@ class Reference:
             f = getattr(self.lib, f"ref_blocks_free_{sfx}")
             f.restype = None
             f.argtypes = [_P]
+        for sfx, sc in (("z", ctypes.c_double), ("c", ctypes.c_float)):
+            f = getattr(self.lib, f"ref_standard_spmv_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, _I64, sc, sc, _P,
+                          _I64, _I64, _SZ, _P, _I64, _I64, _SZ]
+            f = getattr(self.lib, f"ref_standard_spmm_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, _I64, sc, sc, _P,
+                          _I64, _I64, _INT, _I64, _SZ, _P, _I64, _I64, _INT,
+                          _I64, _SZ]
         f = self.lib.ref_convert_compressed_f64
         f.restype = _INT
         f.argtypes = [_INT, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P]
@@ -234,6 +282,14 @@ class Reference:
         ny = rows if op == OP_NONE else cols
         xs = x.ctypes.data + x_offset * x.itemsize
         ys = y.ctypes.data + y_offset * y.itemsize
+        cs = _complex_suffix(val.dtype)
+        if cs is not None:
+            rs = _real_scalar(val.dtype)
+            a = complex(alpha)
+            return getattr(self.lib, f"ref_standard_spmv_{cs}")(
+                fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val),
+                int(ptr[outer]), rs(a.real), rs(a.imag), xs, nx, incx, x.size, ys,
+                ny, incy, y.size)
         return getattr(self.lib, f"ref_standard_spmv_{_suffix(val.dtype)}")(
             fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val),
             int(ptr[outer]), sc(alpha), xs, nx, incx, x.size, ys, ny, incy,
@@ -242,8 +298,17 @@ class Reference:
     def standard_spmm(self, fmt, op, rows, cols, ptr, idx, val, alpha, b,
                       b_rows, b_cols, b_layout, ldb, c, c_rows, c_cols,
                       c_layout, ldc) -> int:
-        sc = _scalar(val.dtype)
         outer = rows if fmt == CSR else cols
+        cs = _complex_suffix(val.dtype)
+        if cs is not None:
+            rs = _real_scalar(val.dtype)
+            a = complex(alpha)
+            return getattr(self.lib, f"ref_standard_spmm_{cs}")(
+                fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val),
+                int(ptr[outer]), rs(a.real), rs(a.imag), _ptr(b), b_rows, b_cols,
+                b_layout, ldb, b.size, _ptr(c), c_rows, c_cols, c_layout, ldc,
+                c.size)
+        sc = _scalar(val.dtype)
         return getattr(self.lib, f"ref_standard_spmm_{_suffix(val.dtype)}")(
             fmt, op, rows, cols, _ptr(ptr), _ptr(idx), _ptr(val),
             int(ptr[outer]), sc(alpha), _ptr(b), b_rows, b_cols, b_layout, ldb,

@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <array>
+#include <complex>
 #include <cstddef>
 #include <cstdint>
 #include <memory>
@@ -387,6 +388,57 @@ int ref_compat_spmv_f32(std::int64_t rows, std::int64_t cols,
 ASC_REF_STANDARD(f64, double)
 ASC_REF_STANDARD(f32, float)
 #undef ASC_REF_STANDARD
+
+// Complex element kinds: arrays are interleaved (re, im) pairs, the layout of
+// std::complex<R>; alpha arrives as its two parts.
+#define ASC_REF_COMPLEX(SUFFIX, R)                                             \
+  int ref_standard_spmv_##SUFFIX(                                              \
+      int format, int op, std::int64_t rows, std::int64_t cols,                \
+      const std::int64_t* ptr, const std::int64_t* idx, const R* val,          \
+      std::int64_t nnz, R alpha_re, R alpha_im, const R* x, std::int64_t nx,   \
+      std::int64_t incx, std::size_t x_storage, R* y, std::int64_t ny,         \
+      std::int64_t incy, std::size_t y_storage) {                              \
+    using C = std::complex<R>;                                                 \
+    const auto* v = reinterpret_cast<const C*>(val);                           \
+    const auto* xc = reinterpret_cast<const C*>(x);                            \
+    auto* yc = reinterpret_cast<C*>(y);                                        \
+    const C alpha(alpha_re, alpha_im);                                         \
+    if (format == 2) {                                                         \
+      return StandardSpmvTyped<C, asc::SparseCompressedFormat::kCsc>(          \
+          op, rows, cols, ptr, idx, v, nnz, alpha, xc, nx, incx, x_storage,    \
+          yc, ny, incy, y_storage);                                            \
+    }                                                                          \
+    return StandardSpmvTyped<C, asc::SparseCompressedFormat::kCsr>(            \
+        op, rows, cols, ptr, idx, v, nnz, alpha, xc, nx, incx, x_storage, yc,  \
+        ny, incy, y_storage);                                                  \
+  }                                                                            \
+  int ref_standard_spmm_##SUFFIX(                                              \
+      int format, int op, std::int64_t rows, std::int64_t cols,                \
+      const std::int64_t* ptr, const std::int64_t* idx, const R* val,          \
+      std::int64_t nnz, R alpha_re, R alpha_im, const R* b,                    \
+      std::int64_t b_rows, std::int64_t b_cols, int b_layout,                  \
+      std::int64_t ldb, std::size_t b_storage, R* c, std::int64_t c_rows,      \
+      std::int64_t c_cols, int c_layout, std::int64_t ldc,                     \
+      std::size_t c_storage) {                                                 \
+    using C = std::complex<R>;                                                 \
+    const auto* v = reinterpret_cast<const C*>(val);                           \
+    const C alpha(alpha_re, alpha_im);                                         \
+    const auto* bc = reinterpret_cast<const C*>(b);                            \
+    auto* cc = reinterpret_cast<C*>(c);                                        \
+    if (format == 2) {                                                         \
+      return StandardSpmmTyped<C, asc::SparseCompressedFormat::kCsc>(          \
+          op, rows, cols, ptr, idx, v, nnz, alpha, bc, b_rows, b_cols,         \
+          b_layout, ldb, b_storage, cc, c_rows, c_cols, c_layout, ldc,         \
+          c_storage);                                                          \
+    }                                                                          \
+    return StandardSpmmTyped<C, asc::SparseCompressedFormat::kCsr>(            \
+        op, rows, cols, ptr, idx, v, nnz, alpha, bc, b_rows, b_cols, b_layout, \
+        ldb, b_storage, cc, c_rows, c_cols, c_layout, ldc, c_storage);         \
+  }
+
+ASC_REF_COMPLEX(z, double)
+ASC_REF_COMPLEX(c, float)
+#undef ASC_REF_COMPLEX
 
 void* ref_blocks_prepare_f64(std::int64_t rows, std::int64_t cols,
                              const std::int64_t* ptr, const std::int64_t* idx,

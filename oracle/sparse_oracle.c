@@ -125,6 +125,86 @@ ORACLE_STANDARD_SPMM(f64, double)
 ORACLE_STANDARD_SPMM(f32, float)
 
 /* ------------------------------------------------------------------------- */
+/* Complex standard SpMV / SpMM: the same loops over interleaved (re, im)
+ * storage, the layout of std::complex<T> (two T, real first).  Each entry
+ * does out += (alpha * v') * in with v' = conj(v) for the conjugate
+ * transpose (blas.h:1653-1665, 1739-1748; MaybeConjugate).  A complex product
+ * (a, b) * (c, d) is (ac - bd, ad + bc) with every product and sum rounded
+ * separately and a sum is component-wise: the value std::complex<T> gives
+ * under GCC without -march (no contraction) whenever the result is not
+ * NaN + NaN i -- only then does C99 Annex G's recovery (__muldc3) differ,
+ * so the oracle, like the tests, covers finite data.                       */
+#define ORACLE_COMPLEX(SUFFIX, T)                                              \
+  static inline void cmul_##SUFFIX(T ar, T ai, T br, T bi, T* r, T* i) {       \
+    const T rr = ar * br;                                                      \
+    const T ii = ai * bi;                                                      \
+    const T ri = ar * bi;                                                      \
+    const T ir = ai * br;                                                      \
+    *r = rr - ii;                                                              \
+    *i = ri + ir;                                                              \
+  }                                                                            \
+  void oracle_complex_spmv_##SUFFIX(int format, int op, int64_t rows,          \
+                                    int64_t cols, const int64_t* ptr,          \
+                                    const int64_t* idx, const T* val, T al_r,  \
+                                    T al_i, const T* x, int64_t incx, T* y,    \
+                                    int64_t incy) {                            \
+    if (al_r == (T)0 && al_i == (T)0) return;                                  \
+    const int64_t outer_extent = format == ORACLE_CSC ? cols : rows;           \
+    for (int64_t o = 0; o < outer_extent; ++o) {                               \
+      for (int64_t p = ptr[o]; p < ptr[o + 1]; ++p) {                         \
+        int64_t row = format == ORACLE_CSC ? idx[p] : o;                       \
+        int64_t col = format == ORACLE_CSC ? o : idx[p];                       \
+        int64_t out = row, in = col;                                           \
+        T vr = val[2 * p], vi = val[2 * p + 1];                                \
+        if (op != ORACLE_OP_NONE) {                                            \
+          out = col;                                                           \
+          in = row;                                                            \
+          if (op == ORACLE_OP_CONJ_TRANSPOSE) vi = -vi;                        \
+        }                                                                      \
+        T tr, ti, pr, pi;                                                      \
+        cmul_##SUFFIX(al_r, al_i, vr, vi, &tr, &ti);                           \
+        cmul_##SUFFIX(tr, ti, x[2 * in * incx], x[2 * in * incx + 1], &pr,     \
+                      &pi);                                                    \
+        y[2 * out * incy] += pr;                                               \
+        y[2 * out * incy + 1] += pi;                                           \
+      }                                                                        \
+    }                                                                          \
+  }                                                                            \
+  void oracle_complex_spmm_##SUFFIX(                                           \
+      int format, int op, int64_t rows, int64_t cols, const int64_t* ptr,      \
+      const int64_t* idx, const T* val, T al_r, T al_i, const T* b,            \
+      int b_layout, int64_t ldb, T* c, int c_layout, int64_t ldc,              \
+      int64_t ncols) {                                                         \
+    if (al_r == (T)0 && al_i == (T)0) return;                                  \
+    const int64_t outer_extent = format == ORACLE_CSC ? cols : rows;           \
+    for (int64_t o = 0; o < outer_extent; ++o) {                               \
+      for (int64_t p = ptr[o]; p < ptr[o + 1]; ++p) {                         \
+        int64_t row = format == ORACLE_CSC ? idx[p] : o;                       \
+        int64_t col = format == ORACLE_CSC ? o : idx[p];                       \
+        int64_t out = row, in = col;                                           \
+        T vr = val[2 * p], vi = val[2 * p + 1];                                \
+        if (op != ORACLE_OP_NONE) {                                            \
+          out = col;                                                           \
+          in = row;                                                            \
+          if (op == ORACLE_OP_CONJ_TRANSPOSE) vi = -vi;                        \
+        }                                                                      \
+        T tr, ti;                                                              \
+        cmul_##SUFFIX(al_r, al_i, vr, vi, &tr, &ti);                           \
+        for (int64_t j = 0; j < ncols; ++j) {                                  \
+          const int64_t bi = dense_at(b_layout, ldb, in, j);                   \
+          const int64_t ci = dense_at(c_layout, ldc, out, j);                  \
+          T pr, pi;                                                            \
+          cmul_##SUFFIX(tr, ti, b[2 * bi], b[2 * bi + 1], &pr, &pi);           \
+          c[2 * ci] += pr;                                                     \
+          c[2 * ci + 1] += pi;                                                 \
+        }                                                                      \
+      }                                                                        \
+    }                                                                          \
+  }
+ORACLE_COMPLEX(z, double)
+ORACLE_COMPLEX(c, float)
+
+/* ------------------------------------------------------------------------- */
 /* Extended-precision companions used to state and check error bounds.
  * For each output o of op(A) (CSR, unit-stride vectors) they return
  *   exact[o] ~= sum_k v_k x_k   (long double accumulation of exact products)

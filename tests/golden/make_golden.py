@@ -27,6 +27,11 @@ into oracle/_ref/libasc_ref.so by oracle/build_oracle.py).  The fixtures pin:
   coordinate -> CSR / CSC conversions (compressed.h:1676-1780) of the
   conversion test's 3 x 4 matrix (tests/sparse/compressed_conversion_test.cc:
   28-36) and of seeded random matrices with empty rows and columns.
+* ``complex_cases.npz`` - complex (Z and C) standard SpMV / SpMM of the
+  reference: the complex 2 x 2 known-answer matrix of
+  tests/sparse/standard_blas_test.cc:177-345 (CSR none, conjugate transpose,
+  CSC none; row-major SpMM, column-major conjugate-transposed CSC SpMM) and a
+  seeded random 300 x 220 matrix for every op.
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -215,6 +220,59 @@ def conversions(ref: Reference) -> dict[str, np.ndarray]:
     return out
 
 
+def complex_cases(ref: Reference) -> dict[str, np.ndarray]:
+    """The reference's complex standard SpMV / SpMM (blas.h:1607-1750 with
+    std::complex elements): the complex 2 x 2 known-answer matrix of
+    standard_blas_test.cc:177-345 and seeded random complex matrices."""
+    out: dict[str, np.ndarray] = {}
+    for dt, tag in ((np.complex128, "z"), (np.complex64, "c")):
+        ptr = np.array([0, 1, 3], np.int64)
+        idx = np.array([0, 0, 1], np.int64)
+        val = np.array([2 + 1j, 1 - 1j, 3 + 0.5j], dt)
+        x = np.array([1 + 2j, -1 + 1j], dt)
+        for name, fmt, op in (("csr_none", CSR, OP_NONE), ("csr_conjt", CSR, 2)):
+            y = np.zeros(2, dt)
+            _check(ref.standard_spmv(fmt, op, 2, 2, ptr, idx, val, 1.0, x, y))
+            out[f"ka_spmv_{name}_{tag}"] = y
+        cptr = np.array([0, 2, 3], np.int64)
+        cidx = np.array([0, 1, 1], np.int64)
+        y = np.zeros(2, dt)
+        _check(ref.standard_spmv(CSC, OP_NONE, 2, 2, cptr, cidx, val, 1.0, x, y))
+        out[f"ka_spmv_csc_none_{tag}"] = y
+        b = np.array([1, 2, 3, 4], dt)
+        c = np.zeros(4, dt)
+        _check(ref.standard_spmm(CSR, OP_NONE, 2, 2, ptr, idx, val, 1.0, b, 2, 2, ROW_MAJOR, 2,
+                                 c, 2, 2, ROW_MAJOR, 2))
+        out[f"ka_spmm_row_{tag}"] = c
+        b = np.array([1, 3, 2, 4], dt)
+        c = np.zeros(4, dt)
+        _check(ref.standard_spmm(CSC, 2, 2, 2, cptr, cidx, val, 1.0, b, 2, 2, COL_MAJOR, 2,
+                                 c, 2, 2, COL_MAJOR, 2))
+        out[f"ka_spmm_csc_col_conjt_{tag}"] = c
+        rng = np.random.default_rng(51 if tag == "z" else 52)
+        a = synthetic.random_csr(rng, 300, 220, 25, np.float64, 0.15)
+        v = (rng.standard_normal(a.nnz) + 1j * rng.standard_normal(a.nnz)).astype(dt)
+        out[f"rand_shape_{tag}"] = np.array([a.rows, a.cols], np.int64)
+        out[f"rand_ptr_{tag}"], out[f"rand_idx_{tag}"], out[f"rand_val_{tag}"] = a.ptr, a.idx, v
+        alpha = 0.75 - 1.25j
+        for op in (OP_NONE, OP_TRANSPOSE, 2):
+            nx = a.cols if op == OP_NONE else a.rows
+            ny = a.rows if op == OP_NONE else a.cols
+            xx = (rng.uniform(-1, 1, nx) + 1j * rng.uniform(-1, 1, nx)).astype(dt)
+            yy = (rng.uniform(-1, 1, ny) + 1j * rng.uniform(-1, 1, ny)).astype(dt)
+            out[f"rand_x_op{op}_{tag}"], out[f"rand_y0_op{op}_{tag}"] = xx, yy.copy()
+            _check(ref.standard_spmv(CSR, op, a.rows, a.cols, a.ptr, a.idx, v, alpha, xx, yy))
+            out[f"rand_y_op{op}_{tag}"] = yy
+            k = 5
+            bb = (rng.uniform(-1, 1, (nx, k)) + 1j * rng.uniform(-1, 1, (nx, k))).astype(dt)
+            cc = (rng.uniform(-1, 1, (ny, k)) + 1j * rng.uniform(-1, 1, (ny, k))).astype(dt)
+            out[f"rand_b_op{op}_{tag}"], out[f"rand_c0_op{op}_{tag}"] = bb, cc.copy()
+            _check(ref.standard_spmm(CSR, op, a.rows, a.cols, a.ptr, a.idx, v, alpha, bb, nx, k,
+                                     ROW_MAJOR, k, cc, ny, k, ROW_MAJOR, k))
+            out[f"rand_c_op{op}_{tag}"] = cc
+    return out
+
+
 def main() -> None:
     build_oracle.build_reference()
     ref = Reference()
@@ -222,7 +280,9 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "random_cases.npz"), **random_cases(ref))
     np.savez_compressed(os.path.join(HERE, "laplacian.npz"), **laplacian(ref))
     np.savez_compressed(os.path.join(HERE, "conversions.npz"), **conversions(ref))
-    for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz", "conversions.npz"):
+    np.savez_compressed(os.path.join(HERE, "complex_cases.npz"), **complex_cases(ref))
+    for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz", "conversions.npz",
+              "complex_cases.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))
 
 

@@ -215,3 +215,42 @@ def test_conversion_matches_reference_directly(restatement, reference):
         want = reference.convert_compressed(to_csc, a.rows, a.cols, a.ptr, a.idx, a.val)
         for x, y in zip(got, want):
             assert _bits_equal(x, y)
+
+
+@pytest.mark.parametrize("tag", ["z", "c"])
+def test_complex_restatement_matches_reference_fixtures(restatement, complex_cases, tag):
+    """Complex standard SpMV / SpMM of the oracle equal the reference's
+    (standard_blas_test.cc:177-345 known answers and random cases)."""
+    from oracle import CSC, CSR, COL_MAJOR, OP_NONE, ROW_MAJOR
+    g = complex_cases
+    dt = np.complex128 if tag == "z" else np.complex64
+    ptr, idx = np.array([0, 1, 3], np.int64), np.array([0, 0, 1], np.int64)
+    val = np.array([2 + 1j, 1 - 1j, 3 + 0.5j], dt)
+    x = np.array([1 + 2j, -1 + 1j], dt)
+    for name, op in (("csr_none", OP_NONE), ("csr_conjt", 2)):
+        y = np.zeros(2, dt)
+        restatement.standard_spmv(CSR, op, 2, 2, ptr, idx, val, 1.0, x, y)
+        assert _bits_equal(y, g[f"ka_spmv_{name}_{tag}"])
+    y = np.zeros(2, dt)
+    restatement.standard_spmv(CSC, OP_NONE, 2, 2, np.array([0, 2, 3]), np.array([0, 1, 1]), val,
+                              1.0, x, y)
+    assert _bits_equal(y, g[f"ka_spmv_csc_none_{tag}"])
+    c = np.zeros(4, dt)
+    restatement.standard_spmm(CSR, OP_NONE, 2, 2, ptr, idx, val, 1.0, np.array([1, 2, 3, 4], dt),
+                              ROW_MAJOR, 2, c, ROW_MAJOR, 2, 2)
+    assert _bits_equal(c, g[f"ka_spmm_row_{tag}"])
+    c = np.zeros(4, dt)
+    restatement.standard_spmm(CSC, 2, 2, 2, np.array([0, 2, 3]), np.array([0, 1, 1]), val, 1.0,
+                              np.array([1, 3, 2, 4], dt), COL_MAJOR, 2, c, COL_MAJOR, 2, 2)
+    assert _bits_equal(c, g[f"ka_spmm_csc_col_conjt_{tag}"])
+    rows, cols = (int(v) for v in g[f"rand_shape_{tag}"])
+    p, i, v = g[f"rand_ptr_{tag}"], g[f"rand_idx_{tag}"], g[f"rand_val_{tag}"]
+    for op in (0, 1, 2):
+        y = g[f"rand_y0_op{op}_{tag}"].copy()
+        restatement.standard_spmv(CSR, op, rows, cols, p, i, v, 0.75 - 1.25j,
+                                  g[f"rand_x_op{op}_{tag}"], y)
+        assert _bits_equal(y, g[f"rand_y_op{op}_{tag}"])
+        c = g[f"rand_c0_op{op}_{tag}"].copy()
+        restatement.standard_spmm(CSR, op, rows, cols, p, i, v, 0.75 - 1.25j,
+                                  g[f"rand_b_op{op}_{tag}"], ROW_MAJOR, 5, c, ROW_MAJOR, 5, 5)
+        assert _bits_equal(c, g[f"rand_c_op{op}_{tag}"])
