@@ -733,7 +733,7 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
   }
   return Launched(ctx,
                   ascb_spmm(ctx->stream, Dtype(m->element_kind), transposed && !planned ? 1 : 0,
-                            &a, c->columns, b->data, b->layout, b->leading_dimension,
+                            ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0, &a, c->columns, b->data, b->layout, b->leading_dimension,
                             const_cast<void*>(c->data), c->layout, c->leading_dimension,
                             alpha_real, ctx->sm_count),
                   "CUDA could not launch the SpMM kernel");

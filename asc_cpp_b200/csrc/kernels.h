@@ -106,8 +106,9 @@ int ascb_complex_spmm(void* stream, int dtype, int mode, int conj, const ascb_cs
                       int64_t ldc, double alpha_re, double alpha_im, int sm_count);
 
 // ---- SpMM: C += alpha * op(A) * B (k right-hand sides) ----
-// transpose = 0: bit-exact stored-order kernel; 1: atomic scatter.
-int ascb_spmm(void* stream, int dtype, int transpose, const ascb_csr* a,
+// transpose = 0: stored-order row kernels (exact = 1: the reference's order
+// and rounding; 0: contracted); 1: atomic scatter.
+int ascb_spmm(void* stream, int dtype, int transpose, int exact, const ascb_csr* a,
               int64_t k, const void* b, int b_layout, int64_t ldb, void* c,
               int c_layout, int64_t ldc, double alpha, int sm_count);
 

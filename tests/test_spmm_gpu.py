@@ -104,3 +104,32 @@ def test_spmm_shape_error(cuda_lib):
                  DenseMatrixView(dev(np.ones(4)), 2, 2))
     assert e.value.code == ErrorCode.kShape
     ctx.close()
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64])
+@pytest.mark.parametrize("k", [4, 8, 12, 32, 128, 200, 6])
+def test_row_major_default_mode_within_bound(cuda_lib, restatement, dt, k):
+    """BACKEND_DEFAULT row-major SpMM (contracted, alpha applied once per
+    output) stays within gamma_{n+2}(|alpha| |A| |B| + |C0|) of the exact
+    product; k not a multiple of the 16-byte chunk takes the scalar kernel."""
+    rng = np.random.default_rng(100 + k)
+    a_h = synthetic.random_csr(rng, 900, 600, 50, dt, 0.1)
+    b = rng.uniform(-1, 1, (a_h.cols, k)).astype(dt)
+    c0 = rng.uniform(-1, 1, (a_h.rows, k)).astype(dt)
+    ctx = context(Determinism.kBackendDefault)
+    a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+    c = dev(c0)
+    CudaSpmm(ctx, SparseBlasTranspose.kNone, -1.5, a,
+             DenseMatrixView(dev(b), a_h.cols, k, writable=False), DenseMatrixView(c, a_h.rows, k))
+    out = host(c)
+    counts = restatement.output_counts(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx)
+    for j in range(k):
+        bj = np.ascontiguousarray(b[:, j])
+        exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
+                                             a_h.val, bj)
+        ref = c0[:, j].astype(np.float64) - 1.5 * exact.astype(np.float64)
+        bound = gamma(counts + 2, dt) * (1.5 * absval.astype(np.float64) +
+                                         np.abs(c0[:, j].astype(np.float64)))
+        err = np.abs(out[:, j].astype(np.float64) - ref)
+        assert np.all(err <= bound + np.finfo(dt).tiny), j
+    ctx.close()
