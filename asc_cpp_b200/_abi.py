@@ -152,6 +152,18 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
     "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
     "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
+    "asc_sb_batch_workspace_size": (ctypes.c_int, [_P, _I64, _SP, ctypes.POINTER(_SZ)]),
+    "asc_sb_batch_create": (ctypes.c_int, [_P, _I64, _SP, _VP, _VP, _P, _SZ,
+                                           ctypes.POINTER(_P)]),
+    "asc_sb_batch_destroy": (ctypes.c_int, [_P]),
+    "asc_sb_batch_set_schedule": (ctypes.c_int, [_P, _P, _I32, _I32]),
+    "asc_sb_batch_get_schedule": (ctypes.c_int, [_P, ctypes.POINTER(_I32),
+                                                 ctypes.POINTER(_I32)]),
+    "asc_sb_batch_spmv": (ctypes.c_int, [_P, _P, _D, _D]),
+    "asc_sb_batch_spmv_per_matrix": (ctypes.c_int, [_P, _P, _D, _D]),
+    "asc_sb_batch_capture": (ctypes.c_int, [_P, _P, _D, _D]),
+    "asc_sb_batch_autotune": (ctypes.c_int, [_P, _P, _D, _D, _I32,
+                                             ctypes.POINTER(ctypes.c_float)]),
     "asc_sb_convert_workspace_size": (ctypes.c_int, [_P, _I64, _I64, _I64, _I32,
                                                      ctypes.POINTER(_SZ)]),
     "asc_sb_convert_compressed": (ctypes.c_int, [_P, _SP, _SP, _P, _SZ]),

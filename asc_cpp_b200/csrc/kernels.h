@@ -85,6 +85,33 @@ int ascb_spmv_seg_alignment(void);
 int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
                   double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
                   int64_t ntiles, int sm_count);
+// ---- batched compat SpMV: many independent CSR matrices, one launch ----
+// One matrix of a batch, as the persistent kernel reads it (device table).
+typedef struct ascb_batch_item {
+  const int64_t* ptr;
+  const int64_t* idx;
+  const void* val;
+  const void* x;        // logical element 0
+  void* y;              // logical element 0
+  int64_t rows;
+  int64_t nnz;
+  int64_t incx;
+  int64_t incy;
+  int64_t tile_base;    // first global tile of this matrix
+  int64_t bound_base;   // first entry of its tile bounds (tile_base + index)
+} ascb_batch_item;
+// Tile bounds of every matrix: bounds[bound_base + k] = first row of tile k,
+// k = 0..tiles (the last entry is rows).  `items` is the device table.
+int ascb_batch_tile_bounds(void* stream, const ascb_batch_item* items, int64_t count,
+                           int64_t* bounds, int64_t total_bounds, int sm_count);
+// Persistent work-queue SpMV over all tiles of the batch: warps take `chunk`
+// tiles at a time from *queue (zero before the launch); ctas_per_sm = 0 uses
+// the occupancy limit.  Index and value arrays must be 16-byte aligned.
+int ascb_spmv_seg_batch(void* stream, int dtype, int exact, int unit,
+                        const ascb_batch_item* items, int64_t count, const int64_t* bounds,
+                        int64_t total_tiles, unsigned long long* queue, int chunk,
+                        int ctas_per_sm, double alpha, double beta, int sm_count);
+
 // Vector CSR: `lanes` (1..32, power of two) threads per row.
 int ascb_spmv_vector(void* stream, int dtype, int form, int lanes,
                      const ascb_csr* a, double alpha, double beta,

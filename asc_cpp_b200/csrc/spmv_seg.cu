@@ -145,6 +145,188 @@ __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
   }
 }
 
+// One tile: rows r0 .. r0 + nr - 1 (nr >= 1), whose ptr entries lane k holds
+// as rb = ptr[r0 + k], re = ptr[r0 + k + 1] (k < nr).  Shared by the
+// single-matrix and the batched kernels.
+template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+__device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t* __restrict__ idx,
+                                         const T* __restrict__ val, const T* __restrict__ x,
+                                         int64_t incx, T* __restrict__ y, int64_t incy, T alpha,
+                                         T beta, int64_t r0, int nr, int64_t rb, int64_t re) {
+  const unsigned lt_mask = (1u << lane) - 1u;
+  // window start alignment: each lane's 8 values and 8 indices start on a
+  // 16-byte boundary (arrays are 16-byte aligned, checked by the host)
+  constexpr int64_t kAlign = sizeof(T) == 8 ? 2 : 4;
+
+  const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
+  const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
+  const int64_t a0 = base / kAlign * kAlign;
+  const int lo = static_cast<int>(base - a0);
+  const int window = static_cast<int>(span < kItems - lo ? span : kItems - lo);
+  const int lim = lo + window;
+  const bool ends_here = span <= window;  // the last row ends in the window
+
+  // row-start bitmap (+ end marker at lim) and nonempty-row table
+  if (lane <= kItems / 32) w.bits[lane] = 0u;
+  __syncwarp();
+  const bool mine = lane < nr;
+  const bool nonempty = mine && re > rb;
+  if (nonempty) {
+    const int s = static_cast<int>(rb - a0);
+    atomicOr(&w.bits[s >> 5], 1u << (s & 31));
+  }
+  if (lane == 0 && ends_here) atomicOr(&w.bits[lim >> 5], 1u << (lim & 31));
+  const unsigned ne_mask = __ballot_sync(0xffffffffu, nonempty);
+  if (nonempty) {
+    const int k = __popc(ne_mask & lt_mask);
+    w.rowid[k] = lane;
+    if (EXACT && STANDARD) w.yinit[k] = at<UNIT>(y, r0 + lane, incy);
+  }
+  if (mine && !nonempty && !STANDARD) {  // empty row: y = alpha*(+0) + beta*y
+    T* yp = &at<UNIT>(y, r0 + lane, incy);
+    *yp = finish<EXACT, STANDARD>(T(0), alpha, beta, yp);
+  }
+  __syncwarp();
+
+  // lane's 8 contiguous positions [8*lane, 8*lane + 8) of the window
+  const int p0 = kPer * lane;
+  const int vlo = lo - p0 < 0 ? 0 : (lo - p0 > kPer ? kPer : lo - p0);
+  const int vhi = lim - p0 < 0 ? 0 : (lim - p0 > kPer ? kPer : lim - p0);
+  const uint32_t vmask = ((1u << vhi) - 1u) & ~((1u << vlo) - 1u);
+  T p[kPer];
+  lane_products<T, EXACT, STANDARD, UNIT>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
+                                          alpha);
+  const uint32_t word = w.bits[lane >> 2];
+  const uint32_t flags = (word >> ((lane & 3) * 8)) & 0xffu;
+  const uint32_t next_word = w.bits[(lane + 1) >> 2];
+  const bool next_start = ((next_word >> (((lane + 1) & 3) * 8)) & 1u) != 0u;
+  // segment ranks: starts strictly before this lane
+  int before = __popc(flags);
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, before, o);
+    if (lane >= o) before += v;
+  }
+  before -= __popc(flags);  // exclusive
+
+  // local segmented sum.  A segment that starts inside the lane is summed
+  // here (in stored order); the lane's first segment, when it continues a
+  // row from earlier lanes, is joined below.
+  const bool has_data = vmask != 0u;
+  int rank = before;  // rows started at or before the current position
+  T acc = T(0);
+  bool first_seg = true;  // still in the segment open at the lane's start
+  T first_val = T(0);
+  int first_rank = -1;
+  int first_end = kPer;   // position where the continued segment closes
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+    if ((flags >> i) & 1u) {
+      if (i > 0 && p0 + i > lo) {  // close the segment before position i
+        if (first_seg) {
+          first_val = acc;
+          first_rank = rank;
+          first_end = i;
+        } else {
+          T* yp = &at<UNIT>(y, r0 + w.rowid[rank - 1], incy);
+          *yp = finish<EXACT, STANDARD>(acc, alpha, beta, yp);
+        }
+      }
+      first_seg = false;
+      ++rank;
+      acc = add<EXACT>(row_init<EXACT, STANDARD>(w.yinit[rank - 1]), p[i]);
+    } else if (!(EXACT && first_seg)) {
+      acc = add<EXACT>(acc, p[i]);
+    }
+  }
+  const bool has_start = flags != 0u;
+  T c;  // this lane's carry out: the running sum of the row open at its end
+  T carry_in = T(0);
+  if (!EXACT) {
+    // segmented scan of the open tails: c = has_start ? acc : c_prev + acc
+    c = acc;
+    bool f = has_start;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const T cu = __shfl_up_sync(0xffffffffu, c, o);
+      const bool fu = __shfl_up_sync(0xffffffffu, f, o);
+      if (lane >= o) {
+        if (!f) c = cu + c;
+        f = f || fu;
+      }
+    }
+    carry_in = __shfl_up_sync(0xffffffffu, c, 1);
+    if (lane == 0) carry_in = T(0);
+    if (first_rank > 0) {  // continued row closed inside this lane
+      T* yp = &at<UNIT>(y, r0 + w.rowid[first_rank - 1], incy);
+      *yp = finish<EXACT, STANDARD>(carry_in + first_val, alpha, beta, yp);
+    }
+  } else {
+    // exact: the running sum is handed lane to lane; a lane whose first
+    // valid position starts a row (or that has no data) needs nothing.
+    bool resolved = !has_data || ((flags >> vlo) & 1u);
+    c = acc;
+    for (int step = 0; step < 32; ++step) {
+      const T cu = __shfl_up_sync(0xffffffffu, c, 1);
+      const bool ru = __shfl_up_sync(0xffffffffu, resolved, 1);
+      if (!resolved && ru) {
+        T s = cu;
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) {
+          if (k >= vlo && k < first_end) s = add_rn(s, p[k]);
+        }
+        if (first_rank > 0) {
+          T* yp = &at<UNIT>(y, r0 + w.rowid[first_rank - 1], incy);
+          *yp = finish<EXACT, STANDARD>(s, alpha, beta, yp);
+          c = acc;
+        } else {
+          c = s;
+        }
+        resolved = true;
+      }
+      if (__all_sync(0xffffffffu, resolved)) break;
+    }
+  }
+  if (has_data && next_start && rank > 0 && p0 + kPer <= lim) {
+    // the open segment closes at the lane end (row start or data end next)
+    T* yp = &at<UNIT>(y, r0 + w.rowid[rank - 1], incy);
+    *yp = finish<EXACT, STANDARD>(c, alpha, beta, yp);
+  }
+  const T carry_out = __shfl_sync(0xffffffffu, c, 31);
+
+  if (!ends_here) {
+    // long last row: the nonzeros past the window
+    T total;
+    if (!EXACT) {
+      T part = T(0);
+      for (int64_t q = base + window + lane; q < base + span; q += 32) {
+        part = fma(ld_stream(val + q), ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)), part);
+      }
+#pragma unroll
+      for (int m = 16; m > 0; m >>= 1) part += shfl_xor(part, m);
+      total = carry_out + part;
+    } else {
+      // 32 products per round, then added in stored order
+      total = carry_out;
+      for (int64_t q0 = base + window; q0 < base + span; q0 += 32) {
+        const int64_t q = q0 + lane;
+        T pv = T(0);
+        if (q < base + span) {
+          pv = product<true, STANDARD>(alpha, ld_stream(val + q),
+                                       ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)));
+        }
+        const int n = static_cast<int>(base + span - q0 < 32 ? base + span - q0 : 32);
+        for (int k = 0; k < n; ++k) total = add_rn(total, __shfl_sync(0xffffffffu, pv, k));
+      }
+    }
+    if (lane == 0) {
+      T* yp = &at<UNIT>(y, r0 + nr - 1, incy);
+      *yp = finish<EXACT, STANDARD>(total, alpha, beta, yp);
+    }
+  }
+  __syncwarp();  // bitmap and row tables are rewritten by the next tile
+}
+
 template <typename T, bool EXACT, bool STANDARD, bool UNIT>
 __global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
 seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
@@ -154,9 +336,6 @@ seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
   __shared__ SegSmem<T> smem_all[kWarpsPerCta];
   const int lane = threadIdx.x & 31;
   SegSmem<T>& w = smem_all[threadIdx.x >> 5];
-  const unsigned lt_mask = (1u << lane) - 1u;
-  // elements per 16-byte chunk of the narrower-aligned array
-  constexpr int64_t kAlign = sizeof(T) == 8 ? 2 : 4;
 
   const int64_t warp_id = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + (threadIdx.x >> 5);
   const int64_t warp_count = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
@@ -203,179 +382,105 @@ seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
       re_n = lane < nr_n ? __ldg(ptr + r0_n + lane + 1) : 0;
     }
     if (nr == 0) continue;
-
-    const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
-    const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
-    const int64_t a0 = base / kAlign * kAlign;
-    const int lo = static_cast<int>(base - a0);
-    const int window = static_cast<int>(span < kItems - lo ? span : kItems - lo);
-    const int lim = lo + window;
-    const bool ends_here = span <= window;  // the last row ends in the window
-
-    // row-start bitmap (+ end marker at lim) and nonempty-row table
-    if (lane <= kItems / 32) w.bits[lane] = 0u;
-    __syncwarp();
-    const bool mine = lane < nr;
-    const bool nonempty = mine && re > rb;
-    if (nonempty) {
-      const int s = static_cast<int>(rb - a0);
-      atomicOr(&w.bits[s >> 5], 1u << (s & 31));
-    }
-    if (lane == 0 && ends_here) atomicOr(&w.bits[lim >> 5], 1u << (lim & 31));
-    const unsigned ne_mask = __ballot_sync(0xffffffffu, nonempty);
-    if (nonempty) {
-      const int k = __popc(ne_mask & lt_mask);
-      w.rowid[k] = lane;
-      if (EXACT && STANDARD) w.yinit[k] = at<UNIT>(y, r0 + lane, incy);
-    }
-    if (mine && !nonempty && !STANDARD) {  // empty row: y = alpha*(+0) + beta*y
-      T* yp = &at<UNIT>(y, r0 + lane, incy);
-      *yp = finish<EXACT, STANDARD>(T(0), alpha, beta, yp);
-    }
-    __syncwarp();
-
-    // lane's 8 contiguous positions [8*lane, 8*lane + 8) of the window
-    const int p0 = kPer * lane;
-    const int vlo = lo - p0 < 0 ? 0 : (lo - p0 > kPer ? kPer : lo - p0);
-    const int vhi = lim - p0 < 0 ? 0 : (lim - p0 > kPer ? kPer : lim - p0);
-    const uint32_t vmask = ((1u << vhi) - 1u) & ~((1u << vlo) - 1u);
-    T p[kPer];
-    lane_products<T, EXACT, STANDARD, UNIT>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
-                                            alpha);
-    const uint32_t word = w.bits[lane >> 2];
-    const uint32_t flags = (word >> ((lane & 3) * 8)) & 0xffu;
-    const uint32_t next_word = w.bits[(lane + 1) >> 2];
-    const bool next_start = ((next_word >> (((lane + 1) & 3) * 8)) & 1u) != 0u;
-    // segment ranks: starts strictly before this lane
-    int before = __popc(flags);
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(0xffffffffu, before, o);
-      if (lane >= o) before += v;
-    }
-    before -= __popc(flags);  // exclusive
-
-    // local segmented sum.  A segment that starts inside the lane is summed
-    // here (in stored order); the lane's first segment, when it continues a
-    // row from earlier lanes, is joined below.
-    const bool has_data = vmask != 0u;
-    int rank = before;  // rows started at or before the current position
-    T acc = T(0);
-    bool first_seg = true;  // still in the segment open at the lane's start
-    T first_val = T(0);
-    int first_rank = -1;
-    int first_end = kPer;   // position where the continued segment closes
-#pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-      if ((flags >> i) & 1u) {
-        if (i > 0 && p0 + i > lo) {  // close the segment before position i
-          if (first_seg) {
-            first_val = acc;
-            first_rank = rank;
-            first_end = i;
-          } else {
-            T* yp = &at<UNIT>(y, r0 + w.rowid[rank - 1], incy);
-            *yp = finish<EXACT, STANDARD>(acc, alpha, beta, yp);
-          }
-        }
-        first_seg = false;
-        ++rank;
-        acc = add<EXACT>(row_init<EXACT, STANDARD>(w.yinit[rank - 1]), p[i]);
-      } else if (!(EXACT && first_seg)) {
-        acc = add<EXACT>(acc, p[i]);
-      }
-    }
-    const bool has_start = flags != 0u;
-    T c;  // this lane's carry out: the running sum of the row open at its end
-    T carry_in = T(0);
-    if (!EXACT) {
-      // segmented scan of the open tails: c = has_start ? acc : c_prev + acc
-      c = acc;
-      bool f = has_start;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const T cu = __shfl_up_sync(0xffffffffu, c, o);
-        const bool fu = __shfl_up_sync(0xffffffffu, f, o);
-        if (lane >= o) {
-          if (!f) c = cu + c;
-          f = f || fu;
-        }
-      }
-      carry_in = __shfl_up_sync(0xffffffffu, c, 1);
-      if (lane == 0) carry_in = T(0);
-      if (first_rank > 0) {  // continued row closed inside this lane
-        T* yp = &at<UNIT>(y, r0 + w.rowid[first_rank - 1], incy);
-        *yp = finish<EXACT, STANDARD>(carry_in + first_val, alpha, beta, yp);
-      }
-    } else {
-      // exact: the running sum is handed lane to lane; a lane whose first
-      // valid position starts a row (or that has no data) needs nothing.
-      bool resolved = !has_data || ((flags >> vlo) & 1u);
-      c = acc;
-      for (int step = 0; step < 32; ++step) {
-        const T cu = __shfl_up_sync(0xffffffffu, c, 1);
-        const bool ru = __shfl_up_sync(0xffffffffu, resolved, 1);
-        if (!resolved && ru) {
-          T s = cu;
-#pragma unroll
-          for (int k = 0; k < kPer; ++k) {
-            if (k >= vlo && k < first_end) s = add_rn(s, p[k]);
-          }
-          if (first_rank > 0) {
-            T* yp = &at<UNIT>(y, r0 + w.rowid[first_rank - 1], incy);
-            *yp = finish<EXACT, STANDARD>(s, alpha, beta, yp);
-            c = acc;
-          } else {
-            c = s;
-          }
-          resolved = true;
-        }
-        if (__all_sync(0xffffffffu, resolved)) break;
-      }
-    }
-    if (has_data && next_start && rank > 0 && p0 + kPer <= lim) {
-      // the open segment closes at the lane end (row start or data end next)
-      T* yp = &at<UNIT>(y, r0 + w.rowid[rank - 1], incy);
-      *yp = finish<EXACT, STANDARD>(c, alpha, beta, yp);
-    }
-    const T carry_out = __shfl_sync(0xffffffffu, c, 31);
-
-    if (!ends_here) {
-      // long last row: the nonzeros past the window
-      T total;
-      if (!EXACT) {
-        T part = T(0);
-        for (int64_t q = base + window + lane; q < base + span; q += 32) {
-          part = fma(ld_stream(val + q), ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)), part);
-        }
-#pragma unroll
-        for (int m = 16; m > 0; m >>= 1) part += shfl_xor(part, m);
-        total = carry_out + part;
-      } else {
-        // 32 products per round, then added in stored order
-        total = carry_out;
-        for (int64_t q0 = base + window; q0 < base + span; q0 += 32) {
-          const int64_t q = q0 + lane;
-          T pv = T(0);
-          if (q < base + span) {
-            pv = product<true, STANDARD>(alpha, ld_stream(val + q),
-                                         ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)));
-          }
-          const int n = static_cast<int>(base + span - q0 < 32 ? base + span - q0 : 32);
-          for (int k = 0; k < n; ++k) total = add_rn(total, __shfl_sync(0xffffffffu, pv, k));
-        }
-      }
-      if (lane == 0) {
-        T* yp = &at<UNIT>(y, r0 + nr - 1, incy);
-        *yp = finish<EXACT, STANDARD>(total, alpha, beta, yp);
-      }
-    }
-    __syncwarp();  // bitmap and row tables are rewritten by the next tile
+    seg_tile<T, EXACT, STANDARD, UNIT>(w, lane, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
+                                      rb, re);
   }
   (void)nnz;
 }
 
-template <typename T, bool EXACT, bool STANDARD, bool UNIT, typename Kernel>
+// ---- batched: many independent matrices in one persistent launch ---------
+
+// Last matrix whose first global tile is <= t (matrices without tiles share
+// their successor's first tile and are skipped this way).
+__device__ __forceinline__ int64_t batch_matrix_of(const ascb_batch_item* __restrict__ items,
+                                                   int64_t count, int64_t t) {
+  int64_t lo = 0, hi = count - 1;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi + 1) >> 1;
+    if (__ldg(&items[mid].tile_base) <= t) {
+      lo = mid;
+    } else {
+      hi = mid - 1;
+    }
+  }
+  return lo;
+}
+
+__global__ void batch_bounds_kernel(const ascb_batch_item* __restrict__ items, int64_t count,
+                                    int64_t* __restrict__ bounds, int64_t total_bounds) {
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t e = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; e < total_bounds;
+       e += step) {
+    int64_t lo = 0, hi = count - 1;  // last matrix with bound_base <= e
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (__ldg(&items[mid].bound_base) <= e) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
+    }
+    const ascb_batch_item& it = items[lo];
+    const int64_t next = lo + 1 < count ? __ldg(&items[lo + 1].bound_base) : total_bounds;
+    const int64_t tiles = next - __ldg(&it.bound_base) - 1;
+    const int64_t k = e - __ldg(&it.bound_base);
+    bounds[e] = k >= tiles ? __ldg(&it.rows)
+                           : first_row_at(it.ptr, __ldg(&it.rows), kRowWeight, k * kItems);
+  }
+}
+
+template <typename T, bool EXACT, bool UNIT>
+__global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
+seg_batch_kernel(const ascb_batch_item* __restrict__ items, int64_t count,
+                 const int64_t* __restrict__ bounds, int64_t total_tiles,
+                 unsigned long long* __restrict__ queue, int chunk, T alpha, T beta) {
+  __shared__ SegSmem<T> smem_all[kWarpsPerCta];
+  const int lane = threadIdx.x & 31;
+  SegSmem<T>& w = smem_all[threadIdx.x >> 5];
+  int64_t tile_lo = 0, tile_hi = 0, bound_base = 0;
+  const int64_t* ptr = nullptr;
+  const int64_t* idx = nullptr;
+  const T* val = nullptr;
+  const T* x = nullptr;
+  T* y = nullptr;
+  int64_t incx = 1, incy = 1;
+  for (;;) {
+    unsigned long long t0 = 0;
+    if (lane == 0) t0 = atomicAdd(queue, static_cast<unsigned long long>(chunk));
+    t0 = __shfl_sync(0xffffffffu, t0, 0);
+    if (t0 >= static_cast<unsigned long long>(total_tiles)) break;
+    const int64_t t1 = static_cast<int64_t>(t0) + chunk < total_tiles
+                           ? static_cast<int64_t>(t0) + chunk : total_tiles;
+    for (int64_t t = static_cast<int64_t>(t0); t < t1; ++t) {
+      if (t < tile_lo || t >= tile_hi) {
+        const int64_t m = batch_matrix_of(items, count, t);
+        const ascb_batch_item& it = items[m];
+        tile_lo = __ldg(&it.tile_base);
+        tile_hi = m + 1 < count ? __ldg(&items[m + 1].tile_base) : total_tiles;
+        bound_base = __ldg(&it.bound_base);
+        ptr = it.ptr;
+        idx = it.idx;
+        val = static_cast<const T*>(it.val);
+        x = static_cast<const T*>(it.x);
+        y = static_cast<T*>(it.y);
+        incx = __ldg(&it.incx);
+        incy = __ldg(&it.incy);
+      }
+      const int64_t k = bound_base + (t - tile_lo);
+      const int64_t r0 = __ldg(bounds + k);
+      const int nr = static_cast<int>(__ldg(bounds + k + 1) - r0);
+      if (nr == 0) continue;
+      const int64_t rb = lane < nr ? __ldg(ptr + r0 + lane) : 0;
+      const int64_t re = lane < nr ? __ldg(ptr + r0 + lane + 1) : 0;
+      seg_tile<T, EXACT, false, UNIT>(w, lane, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
+                                      rb, re);
+    }
+  }
+}
+
+// CTAs per SM at full occupancy, cached per device and per kernel (Tag
+// distinguishes kernels with the same template arguments).
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, int Tag = 0, typename Kernel>
 int resident(Kernel kernel) {
   static int cached[kMaxDevices] = {};
   int device = 0;
@@ -438,3 +543,70 @@ extern "C" int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const
 }
 
 extern "C" int ascb_spmv_seg_alignment(void) { return 16; }
+
+namespace ascb {
+namespace {
+
+template <typename T, bool EXACT, bool UNIT>
+int launch_batch(cudaStream_t s, const ascb_batch_item* items, int64_t count,
+                 const int64_t* bounds, int64_t total_tiles, unsigned long long* queue, int chunk,
+                 int ctas_per_sm, T alpha, T beta, int sm) {
+  auto kernel = seg_batch_kernel<T, EXACT, UNIT>;
+  int per_sm = ctas_per_sm;
+  if (per_sm <= 0) per_sm = resident<T, EXACT, false, UNIT, 1>(kernel);
+  const int64_t warps_needed = (total_tiles + chunk - 1) / chunk;
+  const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
+  const int64_t cap = static_cast<int64_t>(sm > 0 ? sm : 148) * per_sm;
+  const unsigned blocks =
+      static_cast<unsigned>(ctas_needed < 1 ? 1 : (ctas_needed < cap ? ctas_needed : cap));
+  kernel<<<blocks, kThreads, 0, s>>>(items, count, bounds, total_tiles, queue, chunk, alpha, beta);
+  return static_cast<int>(cudaGetLastError());
+}
+
+template <typename T>
+int batch_typed(cudaStream_t s, int exact, int unit, const ascb_batch_item* items, int64_t count,
+                const int64_t* bounds, int64_t total_tiles, unsigned long long* queue, int chunk,
+                int ctas, double alpha, double beta, int sm) {
+  const T a = static_cast<T>(alpha), b = static_cast<T>(beta);
+  if (exact) {
+    return unit ? launch_batch<T, true, true>(s, items, count, bounds, total_tiles, queue, chunk,
+                                              ctas, a, b, sm)
+                : launch_batch<T, true, false>(s, items, count, bounds, total_tiles, queue, chunk,
+                                               ctas, a, b, sm);
+  }
+  return unit ? launch_batch<T, false, true>(s, items, count, bounds, total_tiles, queue, chunk,
+                                             ctas, a, b, sm)
+              : launch_batch<T, false, false>(s, items, count, bounds, total_tiles, queue, chunk,
+                                              ctas, a, b, sm);
+}
+
+}  // namespace
+}  // namespace ascb
+
+extern "C" int ascb_batch_tile_bounds(void* stream, const ascb_batch_item* items, int64_t count,
+                                      int64_t* bounds, int64_t total_bounds, int sm_count) {
+  if (count <= 0 || total_bounds <= 0) return 0;
+  int64_t blocks = (total_bounds + 255) / 256;
+  const int64_t cap = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * 8;
+  if (blocks > cap) blocks = cap;
+  ascb::batch_bounds_kernel<<<static_cast<unsigned>(blocks), 256, 0,
+                              static_cast<cudaStream_t>(stream)>>>(items, count, bounds,
+                                                                  total_bounds);
+  return static_cast<int>(cudaGetLastError());
+}
+
+extern "C" int ascb_spmv_seg_batch(void* stream, int dtype, int exact, int unit,
+                                   const ascb_batch_item* items, int64_t count,
+                                   const int64_t* bounds, int64_t total_tiles,
+                                   unsigned long long* queue, int chunk, int ctas_per_sm,
+                                   double alpha, double beta, int sm_count) {
+  if (count <= 0 || total_tiles <= 0) return 0;
+  if (chunk < 1) chunk = 1;
+  auto s = static_cast<cudaStream_t>(stream);
+  if (dtype == ASCB_F64) {
+    return ascb::batch_typed<double>(s, exact, unit, items, count, bounds, total_tiles, queue,
+                                     chunk, ctas_per_sm, alpha, beta, sm_count);
+  }
+  return ascb::batch_typed<float>(s, exact, unit, items, count, bounds, total_tiles, queue, chunk,
+                                  ctas_per_sm, alpha, beta, sm_count);
+}

@@ -404,3 +404,77 @@ def CudaConvertCoordinates(context: SparseCudaContext, rows: int, columns: int,
         ctypes.byref(dd), ws.data_ptr(), ws.numel()))
     ws.record_stream(context.stream)
     return out
+
+
+# ---- batched SpMV (one persistent launch for many matrices) ----
+
+class CudaBatch:
+    """Binds independent products y_i = alpha*A_i*x_i + beta*y_i and runs them
+    as one persistent launch (asc_sb_batch_*)."""
+
+    def __init__(self, context: SparseCudaContext, matrices: list[CudaCsrArray],
+                 inputs: list[CudaStridedVectorView], outputs: list[CudaStridedVectorView]):
+        self.context = context
+        self._keep = (matrices, inputs, outputs)
+        n = len(matrices)
+        mats = (_abi.SparseDesc * max(n, 1))(*[m.describe() for m in matrices])
+        xs = (_abi.VectorDesc * max(n, 1))(*[x.describe() for x in inputs])
+        ys = (_abi.VectorDesc * max(n, 1))(*[y.describe() for y in outputs])
+        for i in range(n):
+            xs[i].writable = 0
+        size = ctypes.c_size_t()
+        lib = context._lib
+        context.check(lib.asc_sb_batch_workspace_size(context.handle, n, mats,
+                                                      ctypes.byref(size)))
+        self.workspace = torch.empty(max(size.value, 256), dtype=torch.uint8,
+                                     device=torch.device("cuda", context.device))
+        h = ctypes.c_void_p()
+        context.check(lib.asc_sb_batch_create(context.handle, n, mats, xs, ys,
+                                              self.workspace.data_ptr(), size.value,
+                                              ctypes.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def spmv(self, alpha: float, beta: float) -> None:
+        self.context.check(self.context._lib.asc_sb_batch_spmv(
+            self.context.handle, self._h, float(alpha), float(beta)))
+
+    def spmv_per_matrix(self, alpha: float, beta: float) -> None:
+        self.context.check(self.context._lib.asc_sb_batch_spmv_per_matrix(
+            self.context.handle, self._h, float(alpha), float(beta)))
+
+    def capture(self, alpha: float, beta: float) -> None:
+        self.context.check(self.context._lib.asc_sb_batch_capture(
+            self.context.handle, self._h, float(alpha), float(beta)))
+
+    def set_schedule(self, chunk_tiles: int, ctas_per_sm: int = 0) -> None:
+        self.context.check(self.context._lib.asc_sb_batch_set_schedule(
+            self.context.handle, self._h, int(chunk_tiles), int(ctas_per_sm)))
+
+    def schedule(self) -> tuple[int, int]:
+        c, k = ctypes.c_int32(), ctypes.c_int32()
+        rc = self.context._lib.asc_sb_batch_get_schedule(self._h, ctypes.byref(c),
+                                                         ctypes.byref(k))
+        self.context.check(rc)
+        return c.value, k.value
+
+    def autotune(self, alpha: float, beta: float, reps: int = 3) -> float:
+        best = ctypes.c_float()
+        self.context.check(self.context._lib.asc_sb_batch_autotune(
+            self.context.handle, self._h, float(alpha), float(beta), int(reps),
+            ctypes.byref(best)))
+        return best.value
+
+    def close(self) -> None:
+        if self._h is not None and self._h.value:
+            self.context._lib.asc_sb_batch_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

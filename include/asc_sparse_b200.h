@@ -320,6 +320,62 @@ ASC_SB_API int asc_sb_convert_coordinates(asc_sb_context* context,
                                           void* workspace,
                                           size_t workspace_bytes);
 
+/* ---- batched SpMV (no reference counterpart) ------------------------------
+ * A batch binds `count` independent compat products y_i = alpha A_i x_i +
+ * beta y_i (CSR, one element kind: float or double), validated like
+ * asc_sb_csr_spmv when the batch is created.  asc_sb_batch_spmv runs all of
+ * them as ONE launch of a persistent work-queue kernel: warps take row tiles
+ * of any matrix from a global counter, so thousands of uneven matrices share
+ * the GPU without a launch per matrix.  DETERMINISTIC contexts get the
+ * reference's per-row order and rounding, exactly as asc_sb_csr_spmv.  The
+ * batch keeps pointers to the operands: they must stay valid, and no output
+ * may overlap another output or any input of the batch.  The workspace
+ * (device memory, 256-byte aligned, of the queried size) holds the operand
+ * table, the tile bounds and the queue counter for the life of the batch. */
+typedef struct asc_sb_batch asc_sb_batch;
+ASC_SB_API int asc_sb_batch_workspace_size(asc_sb_context* context,
+                                           int64_t count,
+                                           const asc_sb_sparse* matrices,
+                                           size_t* bytes);
+ASC_SB_API int asc_sb_batch_create(asc_sb_context* context, int64_t count,
+                                   const asc_sb_sparse* matrices,
+                                   const asc_sb_vector* inputs,
+                                   const asc_sb_vector* outputs,
+                                   void* workspace, size_t workspace_bytes,
+                                   asc_sb_batch** out);
+ASC_SB_API int asc_sb_batch_destroy(asc_sb_batch* batch);
+/* Schedule of the persistent launch: tiles a warp takes per queue grab
+ * (1..4096) and CTAs per SM (0 = the occupancy limit, else 1..32). */
+ASC_SB_API int asc_sb_batch_set_schedule(asc_sb_context* context,
+                                         asc_sb_batch* batch,
+                                         int32_t chunk_tiles,
+                                         int32_t ctas_per_sm);
+ASC_SB_API int asc_sb_batch_get_schedule(const asc_sb_batch* batch,
+                                         int32_t* chunk_tiles,
+                                         int32_t* ctas_per_sm);
+/* All products of the batch in one launch (a replay of the captured graph
+ * when asc_sb_batch_capture recorded one for the same alpha, beta,
+ * determinism and schedule). */
+ASC_SB_API int asc_sb_batch_spmv(asc_sb_context* context, asc_sb_batch* batch,
+                                 double alpha, double beta);
+/* The same products as one plain-kernel launch per matrix (the baseline). */
+ASC_SB_API int asc_sb_batch_spmv_per_matrix(asc_sb_context* context,
+                                            asc_sb_batch* batch, double alpha,
+                                            double beta);
+/* Records the persistent launch (queue reset + kernel) for these scalars
+ * into a CUDA graph owned by the batch. */
+ASC_SB_API int asc_sb_batch_capture(asc_sb_context* context,
+                                    asc_sb_batch* batch, double alpha,
+                                    double beta);
+/* Times every schedule of the tuning space (`reps` products each, CUDA events
+ * on the context stream), keeps the fastest and returns its time per product.
+ * The products run for real: outputs are written every time, so with
+ * beta != 0 they accumulate. */
+ASC_SB_API int asc_sb_batch_autotune(asc_sb_context* context,
+                                     asc_sb_batch* batch, double alpha,
+                                     double beta, int32_t reps,
+                                     float* best_ms);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif
