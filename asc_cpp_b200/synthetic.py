@@ -211,3 +211,108 @@ def random_csr(rng: np.random.Generator, rows: int, cols: int,
     ptr, idx = _unique_sorted_rows(rng, max(cols, 1), lengths)
     val = rng.standard_normal(int(ptr[-1])).astype(dtype)
     return Csr(rows, cols, ptr, idx, val)
+
+
+def banded_batch_device(count: int = 4096, min_rows: int = 64, max_rows: int = 16_384,
+                        max_half_band: int = 31, fill: float = 0.01, seed: int = 3,
+                        dtype=None, device=None, align: int = 4):
+    """The banded batch generated on the GPU (same family as banded_batch:
+    square n x n, n ~ U{min_rows..max_rows}, half band ~ U{1..max_half_band},
+    round(fill * band nnz) uniform off-band entries, duplicates removed,
+    values N(0,1)), for full-size runs where host generation would be slow.
+
+    Returns a dict of device tensors: ``ptr`` (all matrices' offsets, each
+    starting at 0), ``idx`` and ``val`` (each matrix's entries start at a
+    multiple of ``align`` elements), ``x`` and ``y`` (concatenated, x
+    uniform[-1, 1]), and per-matrix int64 numpy arrays ``rows``, ``nnz``,
+    ``ptr_base``, ``nz_base`` and ``row_base``.  Sizes and bands come from a
+    numpy generator seeded with ``seed``; entries from a torch CUDA generator
+    with the same seed."""
+    import torch
+    dtype = dtype or torch.float64
+    device = device or torch.device("cuda", 0)
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(min_rows, max_rows + 1, size=count).astype(np.int64)
+    bands = rng.integers(1, max_half_band + 1, size=count).astype(np.int64)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    row_base = np.zeros(count + 1, np.int64)
+    np.cumsum(sizes, out=row_base[1:])
+    total_rows = int(row_base[-1])
+    shift = int(max_rows - 1).bit_length()
+    sizes_d = torch.from_numpy(sizes).to(device)
+    bands_d = torch.from_numpy(bands).to(device)
+    row_base_d = torch.from_numpy(row_base).to(device)
+    mat_of_row = torch.repeat_interleave(torch.arange(count, device=device), sizes_d)
+    r = torch.arange(total_rows, device=device) - row_base_d[:-1][mat_of_row]
+    n_of_row = sizes_d[mat_of_row]
+    b_of_row = bands_d[mat_of_row]
+    lo = torch.clamp(r - b_of_row, min=0)
+    hi = torch.minimum(r + b_of_row, n_of_row - 1)
+    band_len = hi - lo + 1
+    del n_of_row, hi
+    band_total = int(band_len.sum())
+    # band keys: global row << shift | column, already sorted
+    start = torch.cumsum(band_len, 0) - band_len
+    grow = torch.repeat_interleave(torch.arange(total_rows, device=device), band_len)
+    col = torch.arange(band_total, device=device) - start[grow] + lo[grow]
+    keys = (grow << shift) | col
+    del grow, col, start, lo
+    band_nnz = torch.zeros(count, dtype=torch.int64, device=device)
+    band_nnz.index_add_(0, mat_of_row, band_len)
+    del band_len, r, b_of_row, mat_of_row
+    n_fill = torch.round(band_nnz.double() * fill).long()
+    fill_total = int(n_fill.sum())
+    if fill_total:
+        fm = torch.repeat_interleave(torch.arange(count, device=device), n_fill)
+        fn = sizes_d[fm]
+        fr = (torch.rand(fill_total, generator=gen, device=device, dtype=torch.float64) * fn).long()
+        fc = (torch.rand(fill_total, generator=gen, device=device, dtype=torch.float64) * fn).long()
+        fr = torch.minimum(fr, fn - 1)
+        fc = torch.minimum(fc, fn - 1)
+        off = (fr - fc).abs() > bands_d[fm]
+        fkeys = ((row_base_d[:-1][fm] + fr) << shift) | fc
+        fkeys = torch.unique(fkeys[off])
+        keys = torch.sort(torch.cat([keys, fkeys])).values
+        del fm, fn, fr, fc, off, fkeys
+    grow = keys >> shift
+    col = keys & ((1 << shift) - 1)
+    del keys
+    counts = torch.bincount(grow, minlength=total_rows)
+    gptr = torch.zeros(total_rows + 1, dtype=torch.int64, device=device)
+    torch.cumsum(counts, 0, out=gptr[1:])
+    del counts, grow
+    nnz_base_plain = gptr[row_base_d].cpu().numpy()
+    nnz = np.diff(nnz_base_plain)
+    # rebased offsets: matrix m's ptr at ptr_base[m] .. ptr_base[m] + n_m
+    ptr_base = row_base[:-1] + np.arange(count, dtype=np.int64)
+    pm = torch.repeat_interleave(torch.arange(count, device=device), sizes_d + 1)
+    local = torch.arange(int(ptr_base[-1] + sizes[-1] + 1), device=device) - \
+        torch.from_numpy(ptr_base).to(device)[pm]
+    grow0 = row_base_d[:-1][pm]
+    ptr = gptr[grow0 + local] - gptr[grow0]
+    del pm, local, grow0
+    # entries moved so that every matrix starts at a multiple of `align`
+    padded = (nnz + align - 1) // align * align
+    nz_base = np.zeros(count + 1, np.int64)
+    np.cumsum(padded, out=nz_base[1:])
+    total_padded = int(nz_base[-1])
+    total_nnz = int(nnz.sum())
+    mat_of_entry = torch.repeat_interleave(torch.arange(count, device=device),
+                                           torch.from_numpy(nnz).to(device))
+    dest = torch.arange(total_nnz, device=device) - \
+        torch.from_numpy(nnz_base_plain[:-1]).to(device)[mat_of_entry] + \
+        torch.from_numpy(nz_base[:-1]).to(device)[mat_of_entry]
+    del mat_of_entry
+    idx = torch.zeros(total_padded, dtype=torch.int64, device=device)
+    idx[dest] = col
+    del col
+    val = torch.zeros(total_padded, dtype=dtype, device=device)
+    val[dest] = torch.randn(total_nnz, generator=gen, device=device,
+                            dtype=torch.float64).to(dtype)
+    del dest, gptr
+    x = (torch.rand(total_rows, generator=gen, device=device, dtype=torch.float64) * 2 - 1).to(dtype)
+    y = torch.zeros(total_rows, dtype=dtype, device=device)
+    torch.cuda.synchronize(device)
+    return {"ptr": ptr, "idx": idx, "val": val, "x": x, "y": y, "rows": sizes, "nnz": nnz,
+            "ptr_base": ptr_base, "nz_base": nz_base[:-1], "row_base": row_base[:-1]}
