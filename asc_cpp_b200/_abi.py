@@ -152,6 +152,17 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
     "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
     "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
+    "asc_sb_selector_param_count": (ctypes.c_int64, [_I32]),
+    "asc_sb_context_set_selector": (ctypes.c_int, [_P, _I32, _P, _P, _P]),
+    "asc_sb_plan_variant": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
+    "asc_sb_plan_autotune": (ctypes.c_int, [_P, _P, _VP, _VP, _I32, _P, _P, _I32, _P]),
+    "asc_sb_matrix_features": (ctypes.c_int, [_P, _SP, _P, _P]),
+    "asc_sb_selector_forward": (ctypes.c_int, [_P, _I32, _P, _P, _I64, _P, _P]),
+    "asc_sb_selector_backward": (ctypes.c_int, [_P, _I32, _P, _P, _I64, _P, _P, _P, _P, _P,
+                                                _P]),
+    "asc_sb_selector_adam": (ctypes.c_int, [_P, _P, _P, _P, _P, _I64, ctypes.c_float,
+                                            ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                            _I32]),
     "asc_sb_batch_workspace_size": (ctypes.c_int, [_P, _I64, _SP, ctypes.POINTER(_SZ)]),
     "asc_sb_batch_create": (ctypes.c_int, [_P, _I64, _SP, _VP, _VP, _P, _SZ,
                                            ctypes.POINTER(_P)]),

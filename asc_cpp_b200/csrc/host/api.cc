@@ -13,6 +13,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "../../../include/asc_sparse_b200.h"
 #include "../kernels.h"
@@ -36,6 +37,11 @@ struct asc_sb_context {
   std::string last_error;
   std::atomic<std::int64_t> launches{0};
   int* status = nullptr;  // device word: kernels record bounded-wait timeouts
+  // installed variant selector: device parameters and scratch, and the
+  // variant (id, lanes) each MLP output stands for
+  int selector_outputs = 0;
+  float* selector = nullptr;
+  std::vector<int> selector_variant, selector_lanes;
 };
 
 // Partitions of one CSR structure, as the kernels consume them.
@@ -56,6 +62,10 @@ struct asc_sb_plan {
   void* t_val = nullptr;
   std::int64_t* t_perm = nullptr;
   Partitions t_part;
+  // variant picked for this matrix (selector or exhaustive autotune);
+  // variant < -1 means none
+  int variant = -2;
+  int lanes = 0;
 };
 
 namespace {
@@ -176,12 +186,21 @@ int AutoLanes(const asc_sb_sparse& m, bool transposed_rows) {
   return lanes;
 }
 
-Choice Choose(const asc_sb_context* ctx, const asc_sb_sparse& m) {
+// Variant for a real CSR product: DETERMINISTIC always takes the bit-exact
+// row-ordered kernels; otherwise a variant forced on the context, else the
+// plan's pick (selector or autotune), else the default, WARP_TILES.
+Choice Choose(const asc_sb_context* ctx, const asc_sb_sparse& m, int plan_variant = -2,
+              int plan_lanes = 0) {
   Choice c;
   if (ctx->determinism == ASC_SB_DETERMINISTIC) return c;  // bit-exact order
   if (ctx->variant != ASC_SB_VARIANT_AUTO) {
     c.variant = ctx->variant;
     c.lanes = ctx->lanes > 0 ? ctx->lanes : AutoLanes(m, false);
+    return c;
+  }
+  if (plan_variant >= 0) {
+    c.variant = plan_variant;
+    c.lanes = plan_lanes > 0 ? plan_lanes : AutoLanes(m, false);
     return c;
   }
   c.variant = ASC_SB_VARIANT_WARP_TILES;
@@ -331,6 +350,55 @@ Status BuildTransposed(asc_sb_context* ctx, const ascb_csr& a, std::size_t eleme
                   "CUDA could not launch the entry permutation kernel");
 }
 
+// ---- variant selector ------------------------------------------------------
+// Device layout of an installed selector (floats): accumulators [0, 16),
+// features [16, 28), hidden units [32, 160), outputs [160, 224), the pick
+// (an int) at 224, parameters from 256 on.
+constexpr int kSelAcc = 0, kSelFeatures = 16, kSelHidden = 32, kSelOut = 160, kSelPick = 224,
+              kSelParams = 256, kSelMaxOutputs = 64;
+
+// Runs features -> MLP -> argmin for the plan's matrix and records the
+// variant the selector's best output stands for.  Synchronizes the stream.
+Status SelectVariant(asc_sb_context* ctx, asc_sb_plan* plan) {
+  float* base = ctx->selector;
+  const ascb_csr a = AsCsr(plan->matrix, plan->matrix.format == ASC_SB_CSC);
+  int rc = ascb_matrix_features(
+      ctx->stream, &a, static_cast<int>(ascb::host::ElementBytes(plan->matrix.element_kind)),
+      reinterpret_cast<unsigned long long*>(base + kSelAcc), base + kSelFeatures, ctx->sm_count);
+  if (rc == 0) {
+    rc = ascb_mlp_forward(ctx->stream, ctx->selector_outputs, base + kSelParams,
+                          base + kSelFeatures, 1, base + kSelHidden, base + kSelOut);
+  }
+  if (rc == 0) {
+    rc = ascb_argmin(ctx->stream, base + kSelOut, ctx->selector_outputs,
+                     reinterpret_cast<int*>(base + kSelPick));
+  }
+  ctx->launches.fetch_add(6, std::memory_order_relaxed);
+  int pick = 0;
+  cudaError_t e = static_cast<cudaError_t>(rc);
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(&pick, base + kSelPick, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+  }
+  const cudaError_t sync = cudaStreamSynchronize(ctx->stream);
+  if (e == cudaSuccess) e = sync;
+  if (e != cudaSuccess || pick < 0 || pick >= ctx->selector_outputs) {
+    (void)cudaGetLastError();
+    return {ASC_SB_PROVIDER, std::string("CUDA could not run the variant selector: ") +
+                                 cudaGetErrorString(e)};
+  }
+  plan->variant = ctx->selector_variant[static_cast<std::size_t>(pick)];
+  plan->lanes = ctx->selector_lanes[static_cast<std::size_t>(pick)];
+  return Status::Ok();
+}
+
+bool ValidVariant(int variant, int lanes) {
+  if (variant == ASC_SB_VARIANT_VECTOR) {
+    return lanes >= 1 && lanes <= 32 && (lanes & (lanes - 1)) == 0;
+  }
+  return variant == ASC_SB_VARIANT_ROW_ORDERED || variant == ASC_SB_VARIANT_WARP_TILES ||
+         variant == ASC_SB_VARIANT_MERGE_PATH;
+}
+
 struct CompatOperands {
   SparseBytes matrix_bytes;
   Span x_span, y_span;
@@ -419,6 +487,7 @@ int asc_sb_context_destroy(asc_sb_context* ctx) {
   (void)cudaStreamSynchronize(ctx->stream);
   if (ctx->owns_stream) (void)cudaStreamDestroy(ctx->stream);
   if (ctx->status != nullptr) (void)cudaFree(ctx->status);
+  if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
   delete ctx;
   return ASC_SB_OK;
 }
@@ -638,7 +707,8 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
                     "CUDA could not launch the complex SpMV kernel");
   }
   if (!transposed) {
-    const Choice choice = Choose(ctx, m);
+    const Choice choice = plan != nullptr ? Choose(ctx, m, plan->variant, plan->lanes)
+                                          : Choose(ctx, m);
     return RunCsr(ctx, choice, ASCB_STANDARD, a, dtype, alpha, 0.0, xv, yv, nullptr,
                   plan != nullptr ? &plan->part : nullptr);
   }
@@ -810,6 +880,10 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
                         reinterpret_cast<std::int64_t*>(ws + l.outer_of));
     if (s.ok()) s = BuildPartitions(ctx, TransposedCsr(*plan), ws + l.t_part, &plan->t_part);
   }
+  if (s.ok() && ctx->selector != nullptr && ctx->determinism != ASC_SB_DETERMINISTIC &&
+      ctx->variant == ASC_SB_VARIANT_AUTO && RealKind(m->element_kind)) {
+    s = SelectVariant(ctx, plan);
+  }
   if (!s.ok()) {
     delete plan;
     return Finish(ctx, s);
@@ -852,7 +926,7 @@ int asc_sb_plan_csr_spmv(asc_sb_context* ctx, const asc_sb_plan* plan, double al
   if (!s.ok()) return Finish(ctx, s);
   if (plan->matrix.rows == 0) return Finish(ctx, Status::Ok());
   const ascb_csr a = AsCsr(plan->matrix, false);
-  const Choice choice = Choose(ctx, plan->matrix);
+  const Choice choice = Choose(ctx, plan->matrix, plan->variant, plan->lanes);
   s = RunCsr(ctx, choice, ASCB_COMPAT, a, Dtype(plan->matrix.element_kind), alpha, beta,
              AsVec(*x), AsVec(*y), nullptr, &plan->part);
   return Finish(ctx, s);
@@ -1076,6 +1150,201 @@ int asc_sb_convert_coordinates(asc_sb_context* ctx, const int64_t* coordinates,
                    ctx->sm_count),
                "CUDA could not launch the entry permutation kernel");
   return Finish(ctx, s);
+}
+
+// ---------------------------------------------------------------------------
+// Learned variant selector.
+
+int64_t asc_sb_selector_param_count(int32_t n_variants) {
+  return n_variants >= 1 && n_variants <= kSelMaxOutputs ? ascb_mlp_param_count(n_variants) : -1;
+}
+
+int asc_sb_context_set_selector(asc_sb_context* ctx, int32_t n_variants, const float* params,
+                                const int32_t* variants, const int32_t* lanes) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  if (params == nullptr) {  // remove
+    (void)cudaStreamSynchronize(ctx->stream);
+    if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
+    ctx->selector = nullptr;
+    ctx->selector_outputs = 0;
+    return Finish(ctx, Status::Ok());
+  }
+  if (n_variants < 1 || n_variants > kSelMaxOutputs || variants == nullptr || lanes == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "selector arguments are invalid"));
+  }
+  for (int i = 0; i < n_variants; ++i) {
+    if (!ValidVariant(variants[i], variants[i] == ASC_SB_VARIANT_VECTOR ? lanes[i] : 1)) {
+      return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "selector names an unknown variant"));
+    }
+  }
+  const std::size_t count = static_cast<std::size_t>(ascb_mlp_param_count(n_variants));
+  const std::size_t bytes = (kSelParams + count) * sizeof(float);
+  (void)cudaStreamSynchronize(ctx->stream);
+  if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
+  ctx->selector = nullptr;
+  float* dev = nullptr;
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&dev), bytes);
+  if (e == cudaSuccess) {
+    e = cudaMemcpy(dev + kSelParams, params, count * sizeof(float), cudaMemcpyHostToDevice);
+  }
+  if (e != cudaSuccess) {
+    if (dev != nullptr) (void)cudaFree(dev);
+    (void)cudaGetLastError();
+    return Finish(ctx, {ASC_SB_ALLOCATION, std::string("could not install the selector: ") +
+                                               cudaGetErrorString(e)});
+  }
+  ctx->selector = dev;
+  ctx->selector_outputs = n_variants;
+  ctx->selector_variant.assign(variants, variants + n_variants);
+  ctx->selector_lanes.assign(lanes, lanes + n_variants);
+  return Finish(ctx, Status::Ok());
+}
+
+int asc_sb_plan_variant(const asc_sb_plan* plan, int32_t* variant, int32_t* lanes) {
+  if (plan == nullptr || variant == nullptr || lanes == nullptr) return ASC_SB_INVALID_ARGUMENT;
+  *variant = plan->variant >= -1 ? plan->variant : ASC_SB_VARIANT_AUTO;
+  *lanes = plan->lanes;
+  return ASC_SB_OK;
+}
+
+int asc_sb_plan_autotune(asc_sb_context* ctx, asc_sb_plan* plan, const asc_sb_vector* x,
+                         const asc_sb_vector* y, int32_t count, const int32_t* variants,
+                         const int32_t* lanes, int32_t reps, float* ms) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr || count < 1 || variants == nullptr || lanes == nullptr || reps < 1) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "autotune arguments are invalid"));
+  }
+  for (int i = 0; i < count; ++i) {
+    if (!ValidVariant(variants[i], variants[i] == ASC_SB_VARIANT_VECTOR ? lanes[i] : 1)) {
+      return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "autotune names an unknown variant"));
+    }
+  }
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  CompatOperands ops;
+  s = ValidateCompat(ctx, &plan->matrix, x, y, &ops);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan->matrix.rows == 0) return Finish(ctx, Status::Ok());
+  const ascb_csr a = AsCsr(plan->matrix, false);
+  const int dtype = Dtype(plan->matrix.element_kind);
+  cudaEvent_t start = nullptr, stop = nullptr;
+  cudaError_t e = cudaEventCreate(&start);
+  if (e == cudaSuccess) e = cudaEventCreate(&stop);
+  int best = -1;
+  float best_ms = 0.0f;
+  for (int i = 0; i < count && e == cudaSuccess && s.ok(); ++i) {
+    Choice c;
+    c.variant = variants[i];
+    c.lanes = lanes[i];
+    // one warm-up, then `reps` timed products y = A x
+    s = RunCsr(ctx, c, ASCB_COMPAT, a, dtype, 1.0, 0.0, AsVec(*x), AsVec(*y), nullptr,
+               &plan->part);
+    if (s.ok()) e = cudaEventRecord(start, ctx->stream);
+    for (int r = 0; r < reps && s.ok() && e == cudaSuccess; ++r) {
+      s = RunCsr(ctx, c, ASCB_COMPAT, a, dtype, 1.0, 0.0, AsVec(*x), AsVec(*y), nullptr,
+                 &plan->part);
+    }
+    if (s.ok() && e == cudaSuccess) e = cudaEventRecord(stop, ctx->stream);
+    if (s.ok() && e == cudaSuccess) e = cudaEventSynchronize(stop);
+    float t = 0.0f;
+    if (s.ok() && e == cudaSuccess) e = cudaEventElapsedTime(&t, start, stop);
+    t /= static_cast<float>(reps);
+    if (ms != nullptr) ms[i] = t;
+    if (s.ok() && e == cudaSuccess && (best < 0 || t < best_ms)) {
+      best = i;
+      best_ms = t;
+    }
+  }
+  if (start != nullptr) (void)cudaEventDestroy(start);
+  if (stop != nullptr) (void)cudaEventDestroy(stop);
+  if (!s.ok()) return Finish(ctx, s);
+  if (e != cudaSuccess) {
+    (void)cudaStreamSynchronize(ctx->stream);
+    (void)cudaGetLastError();
+    return Finish(ctx, {ASC_SB_PROVIDER,
+                        std::string("CUDA failed while autotuning: ") + cudaGetErrorString(e)});
+  }
+  plan->variant = variants[best];
+  plan->lanes = lanes[best];
+  return Finish(ctx, Status::Ok());
+}
+
+int asc_sb_matrix_features(asc_sb_context* ctx, const asc_sb_sparse* m, float* features,
+                           void* scratch) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (m == nullptr || features == nullptr || scratch == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "feature arguments cannot be null"));
+  }
+  SparseBytes mb;
+  s = ascb::host::ValidateSparse(*m, ctx->device, &mb);
+  if (!s.ok()) return Finish(ctx, s);
+  const ascb_csr a = AsCsr(*m, m->format == ASC_SB_CSC);
+  return Finish(ctx, Launched(ctx,
+                              ascb_matrix_features(
+                                  ctx->stream, &a,
+                                  static_cast<int>(ascb::host::ElementBytes(m->element_kind)),
+                                  static_cast<unsigned long long*>(scratch), features,
+                                  ctx->sm_count),
+                              "CUDA could not launch the feature kernels"));
+}
+
+int asc_sb_selector_forward(asc_sb_context* ctx, int32_t n_variants, const float* params,
+                            const float* x, int64_t batch, float* hidden, float* y) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (n_variants < 1 || n_variants > kSelMaxOutputs || batch < 0 ||
+      (batch > 0 && (params == nullptr || x == nullptr || hidden == nullptr || y == nullptr))) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "selector forward arguments are invalid"));
+  }
+  return Finish(ctx, Launched(ctx, ascb_mlp_forward(ctx->stream, n_variants, params, x, batch,
+                                                    hidden, y),
+                              "CUDA could not launch the selector forward kernels"));
+}
+
+int asc_sb_selector_backward(asc_sb_context* ctx, int32_t n_variants, const float* params,
+                             const float* x, int64_t batch, const float* hidden, const float* y,
+                             const float* target, float* grads, float* loss, float* scratch) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (n_variants < 1 || n_variants > kSelMaxOutputs || batch < 0 ||
+      (batch > 0 && (params == nullptr || x == nullptr || hidden == nullptr || y == nullptr ||
+                     target == nullptr || grads == nullptr || scratch == nullptr))) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "selector backward arguments are invalid"));
+  }
+  return Finish(ctx, Launched(ctx,
+                              ascb_mlp_backward(ctx->stream, n_variants, params, x, batch, hidden,
+                                                y, target, grads, loss, scratch),
+                              "CUDA could not launch the selector backward kernels"));
+}
+
+int asc_sb_selector_adam(asc_sb_context* ctx, float* params, const float* grads, float* m,
+                         float* v, int64_t n, float lr, float beta1, float beta2, float eps,
+                         int32_t step) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (n < 0 || step < 1 ||
+      (n > 0 && (params == nullptr || grads == nullptr || m == nullptr || v == nullptr))) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Adam arguments are invalid"));
+  }
+  return Finish(ctx, Launched(ctx,
+                              ascb_adam_step(ctx->stream, params, grads, m, v, n, lr, beta1,
+                                             beta2, eps, step),
+                              "CUDA could not launch the Adam kernel"));
 }
 
 }  // extern "C"

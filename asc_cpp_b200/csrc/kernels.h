@@ -112,6 +112,25 @@ int ascb_spmv_seg_batch(void* stream, int dtype, int exact, int unit,
                         int64_t total_tiles, unsigned long long* queue, int chunk,
                         int ctas_per_sm, double alpha, double beta, int sm_count);
 
+// ---- learned variant selector (features + MLP cost model) ----
+#define ASCB_SELECTOR_FEATURES 12
+#define ASCB_SELECTOR_HIDDEN 64
+int64_t ascb_mlp_param_count(int n_variants);
+// acc: 8 device uint64 of scratch; features: 12 device floats.
+int ascb_matrix_features(void* stream, const ascb_csr* a, int element_bytes,
+                         unsigned long long* acc, float* features, int sm_count);
+// hidden: batch * 128 floats (both hidden layers, kept for the backward pass).
+int ascb_mlp_forward(void* stream, int n_variants, const float* params, const float* x,
+                     int64_t batch, float* hidden, float* y);
+// grads: ascb_mlp_param_count floats; loss (nullable): batch floats;
+// scratch: batch * (n_variants + 128) floats.
+int ascb_mlp_backward(void* stream, int n_variants, const float* params, const float* x,
+                      int64_t batch, const float* hidden, const float* y, const float* target,
+                      float* grads, float* loss, float* scratch);
+int ascb_adam_step(void* stream, float* params, const float* grads, float* m, float* v,
+                   int64_t n, float lr, float beta1, float beta2, float eps, int step);
+int ascb_argmin(void* stream, const float* y, int n, int* out);
+
 // Vector CSR: `lanes` (1..32, power of two) threads per row.
 int ascb_spmv_vector(void* stream, int dtype, int form, int lanes,
                      const ascb_csr* a, double alpha, double beta,

@@ -320,6 +320,70 @@ ASC_SB_API int asc_sb_convert_coordinates(asc_sb_context* context,
                                           void* workspace,
                                           size_t workspace_bytes);
 
+/* ---- learned variant selector (no reference counterpart) ------------------
+ * Twelve features of a matrix (hand-written CUDA kernels) feed a small MLP
+ * cost model (12 -> 64 -> 64 -> V, FP32, ReLU) whose output v estimates the
+ * log run time of variant v relative to the matrix's mean; the smallest wins.
+ * A selector installed on a context picks the variant of every plan created
+ * on it in BACKEND_DEFAULT mode with variant AUTO (DETERMINISTIC products
+ * always run the bit-exact kernels, so the selector never changes numerics
+ * beyond each variant's stated bound).  The training entry points run the
+ * MLP's forward pass, backward pass and Adam update on the GPU.
+ * Features: log2(1 + rows), log2(1 + columns), log2(1 + nnz),
+ * log2(1 + mean row length), log2(1 + max row length), log2(1 + coefficient
+ * of variation of row length), max |column - row| / columns, mean |column -
+ * row| / columns, diagonal entries / min(rows, columns), nnz / (8 * runs of
+ * entries in one 8-column block), empty rows / rows, 1 if double else 0. */
+#define ASC_SB_SELECTOR_FEATURES 12
+#define ASC_SB_SELECTOR_HIDDEN 64
+/* Parameter count for V outputs (1..64), -1 otherwise.  Layout: W1[64][12]
+ * b1[64] W2[64][64] b2[64] W3[V][64] b3[V], row-major, FP32. */
+ASC_SB_API int64_t asc_sb_selector_param_count(int32_t n_variants);
+/* Installs a trained selector (host parameters, copied) whose output i
+ * stands for variant variants[i] with lanes[i]; params = NULL removes it. */
+ASC_SB_API int asc_sb_context_set_selector(asc_sb_context* context,
+                                           int32_t n_variants,
+                                           const float* params,
+                                           const int32_t* variants,
+                                           const int32_t* lanes);
+/* Variant recorded in a plan (selector or autotune); AUTO if none. */
+ASC_SB_API int asc_sb_plan_variant(const asc_sb_plan* plan, int32_t* variant,
+                                   int32_t* lanes);
+/* Exhaustive autotune, the selector's fallback and judge: times y = A x with
+ * each candidate (one warm-up, `reps` timed runs, CUDA events on the context
+ * stream), writes the mean times to ms[count] (nullable) and records the
+ * fastest in the plan.  y is overwritten. */
+ASC_SB_API int asc_sb_plan_autotune(asc_sb_context* context, asc_sb_plan* plan,
+                                    const asc_sb_vector* input,
+                                    const asc_sb_vector* output, int32_t count,
+                                    const int32_t* variants,
+                                    const int32_t* lanes, int32_t reps,
+                                    float* ms);
+/* The twelve features of a device matrix into `features` (12 device floats);
+ * `scratch` is 64 bytes of device memory, 8-byte aligned. */
+ASC_SB_API int asc_sb_matrix_features(asc_sb_context* context,
+                                      const asc_sb_sparse* matrix,
+                                      float* features, void* scratch);
+/* Training kernels (device pointers): forward keeps both hidden layers in
+ * hidden[batch][128]; backward writes the MSE gradient of every parameter
+ * to grads, per-sample losses to loss (nullable), using
+ * scratch[batch][V + 128]; Adam updates params, m and v in place. */
+ASC_SB_API int asc_sb_selector_forward(asc_sb_context* context,
+                                       int32_t n_variants, const float* params,
+                                       const float* x, int64_t batch,
+                                       float* hidden, float* y);
+ASC_SB_API int asc_sb_selector_backward(asc_sb_context* context,
+                                        int32_t n_variants,
+                                        const float* params, const float* x,
+                                        int64_t batch, const float* hidden,
+                                        const float* y, const float* target,
+                                        float* grads, float* loss,
+                                        float* scratch);
+ASC_SB_API int asc_sb_selector_adam(asc_sb_context* context, float* params,
+                                    const float* grads, float* m, float* v,
+                                    int64_t n, float lr, float beta1,
+                                    float beta2, float eps, int32_t step);
+
 /* ---- batched SpMV (no reference counterpart) ------------------------------
  * A batch binds `count` independent compat products y_i = alpha A_i x_i +
  * beta y_i (CSR, one element kind: float or double), validated like
