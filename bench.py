@@ -358,6 +358,144 @@ def run_gpu(args, rank, world):
     return out
 
 
+# ---- further workloads (evidence for the other configurations) -------------
+
+EXTRA = ("spmv_powerlaw_4M_f32", "spmv_t_powerlaw_4M_f64", "spmv_t_powerlaw_4M_f32",
+         "spmm_stencil_k8", "spmm_stencil_k32", "spmm_stencil_k128",
+         "spmm_block_k8", "spmm_block_k32", "spmm_block_k128", "batched_banded_4096")
+
+
+def _timer(stream, steps, warmup):
+    import torch
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        stream.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        stop = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(steps):
+            fn()
+        stop.record(stream)
+        stop.synchronize()
+        return start.elapsed_time(stop) / steps
+    return timed
+
+
+def run_extra(args):
+    """One JSON line for a workload other than the headline: the same keys,
+    both numerical modes timed, the faster one as `value`."""
+    import torch
+    from asc_cpp_b200 import synthetic
+    from asc_cpp_b200._abi import PLAN_TRANSPOSE, Determinism, SparseBlasTranspose
+    from asc_cpp_b200 import sparse_cuda as sc
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    timed = _timer(stream, args.steps, args.warmup)
+    ctx = sc.SparseCudaContext.Create(0, stream=stream)
+    peak, peak_kind = _peaks()
+    w = args.workload
+    detail, extra_cfg = {}, {}
+    if w.startswith("spmv"):
+        transpose = "_t_" in w
+        dt = np.float32 if w.endswith("f32") else np.float64
+        a_h = synthetic.power_law(4_194_304, 16.0, 1.5, 65_536, seed=1, dtype=dt)
+        es = np.dtype(dt).itemsize
+        with torch.cuda.stream(stream):
+            A = sc.CudaCsrArray(a_h.rows, a_h.cols, torch.from_numpy(a_h.ptr).to(dev),
+                                torch.from_numpy(a_h.idx).to(dev), torch.from_numpy(a_h.val).to(dev))
+            x = (torch.rand(a_h.rows if transpose else a_h.cols, device=dev,
+                            dtype=torch.float64) * 2 - 1).to(A.values.dtype)
+            y = torch.zeros(a_h.cols if transpose else a_h.rows, device=dev, dtype=A.values.dtype)
+        stream.synchronize()
+        xv, yv = sc.CudaStridedVectorView(x, x.numel(), writable=False), sc.CudaStridedVectorView(y, y.numel())
+        t0 = time.time()
+        plan = sc.CsrPlan(ctx, A, PLAN_TRANSPOSE if transpose else 0)
+        stream.synchronize()
+        extra_cfg["plan_create_s"] = round(time.time() - t0, 3)
+        op = SparseBlasTranspose.kTranspose if transpose else SparseBlasTranspose.kNone
+        byts = a_h.nnz * (es + 8) + (a_h.rows + 1) * 8 + (a_h.rows + a_h.cols) * es
+        if transpose:
+            byts = a_h.nnz * (es + 8) + (a_h.cols + 1) * 8 + (a_h.rows + a_h.cols) * es
+        for name, det, use_plan in (("deterministic_plan", Determinism.kDeterministic, True),
+                                    ("default_plan", Determinism.kBackendDefault, True),
+                                    ("default_scatter", Determinism.kBackendDefault, False)):
+            if not transpose and name == "default_scatter":
+                continue
+            ctx.set_determinism(det)
+            ms = timed(lambda: sc.CudaSpmv(ctx, op, 1.0, A, xv, yv, plan=plan if use_plan else None))
+            detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1)}
+        plan.close()
+        dtype_s = "f32" if dt == np.float32 else "f64"
+        extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "op": "transpose" if transpose else "none"})
+    elif w.startswith("spmm"):
+        k = int(w.rsplit("_k", 1)[1])
+        a_h = synthetic.stencil_27(128) if "stencil" in w else synthetic.block_sparse()
+        with torch.cuda.stream(stream):
+            A = sc.CudaCsrArray(a_h.rows, a_h.cols, torch.from_numpy(a_h.ptr).to(dev),
+                                torch.from_numpy(a_h.idx).to(dev), torch.from_numpy(a_h.val).to(dev))
+            g = torch.Generator(device=dev)
+            g.manual_seed(2)
+            B = torch.randn(a_h.cols, k, generator=g, device=dev, dtype=torch.float32)
+            C = torch.zeros(a_h.rows, k, device=dev, dtype=torch.float32)
+        stream.synchronize()
+        byts = a_h.nnz * 12 + (a_h.rows + 1) * 8 + 2 * a_h.rows * k * 4
+        flops = 2 * a_h.nnz * k
+        bv = sc.DenseMatrixView(B, a_h.cols, k, writable=False)
+        cv = sc.DenseMatrixView(C, a_h.rows, k)
+        for name, det in (("deterministic", Determinism.kDeterministic),
+                          ("default", Determinism.kBackendDefault)):
+            ctx.set_determinism(det)
+            ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv))
+            detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
+                            "gflops": round(flops / ms / 1e6, 1)}
+        dtype_s = "f32"
+        extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "k": k, "layout": "row-major, ld=k"})
+    else:  # batched
+        g = synthetic.banded_batch_device(4096)
+        mats, xs, ys = [], [], []
+        for m in range(4096):
+            n, z = int(g["rows"][m]), int(g["nnz"][m])
+            pb, nb, rb = int(g["ptr_base"][m]), int(g["nz_base"][m]), int(g["row_base"][m])
+            mats.append(sc.CudaCsrArray(n, n, g["ptr"][pb:pb + n + 1], g["idx"][nb:nb + z],
+                                        g["val"][nb:nb + z]))
+            xs.append(sc.CudaStridedVectorView(g["x"][rb:rb + n], n, writable=False))
+            ys.append(sc.CudaStridedVectorView(g["y"][rb:rb + n], n))
+        batch = sc.CudaBatch(ctx, mats, xs, ys)
+        byts = int((g["nnz"] * 16 + (g["rows"] + 1) * 8 + 2 * g["rows"] * 8).sum())
+        for name, det in (("deterministic", Determinism.kDeterministic),
+                          ("default", Determinism.kBackendDefault)):
+            ctx.set_determinism(det)
+            batch.set_schedule(4, 0)
+            per = _timer(stream, max(3, args.steps // 10), args.warmup)(
+                lambda: batch.spmv_per_matrix(1.0, 0.0))
+            batch.autotune(1.0, 0.0, 3)
+            batch.capture(1.0, 0.0)
+            ms = timed(lambda: batch.spmv(1.0, 0.0))
+            detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
+                            "per_matrix_ms": round(per, 3), "speedup_vs_per_matrix": round(per / ms, 2),
+                            "schedule": batch.schedule()}
+        batch.close()
+        dtype_s = "f64"
+        extra_cfg.update({"matrices": 4096, "rows": int(g["rows"].sum()), "nnz": int(g["nnz"].sum())})
+    best = min(detail, key=lambda k: detail[k]["ms"])
+    ms = detail[best]["ms"]
+    gbs = byts / ms / 1e6
+    out = {"metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": 1,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype_s,
+           "data": "synthetic", "config": {"workload": w, "bytes_per_step": int(byts),
+                                           "best_mode": best, **extra_cfg},
+           "roofline": {"bound": "hbm", "achieved": round(gbs, 2), "peak": peak, "unit": "GB/s",
+                        "frac": round(gbs / peak, 4), "traffic": None, "peak_kind": peak_kind},
+           "detail": detail}
+    ctx.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -366,12 +504,16 @@ def main():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--probe", default=None,
                    help="profiling aid: run 3 launches of one variant and exit")
+    p.add_argument("--workload", default=WORKLOAD, choices=(WORKLOAD,) + EXTRA,
+                   help="another configuration's workload (one GPU, this library only)")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = _env_int("RANK", 0)
     world = _env_int("WORLD_SIZE", 1)
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload != WORKLOAD:
+        return run_extra(args)
     import torch.distributed as dist
     if world > 1:
         import datetime

@@ -254,3 +254,36 @@ def test_complex_restatement_matches_reference_fixtures(restatement, complex_cas
         restatement.standard_spmm(CSR, op, rows, cols, p, i, v, 0.75 - 1.25j,
                                   g[f"rand_b_op{op}_{tag}"], ROW_MAJOR, 5, c, ROW_MAJOR, 5, 5)
         assert _bits_equal(c, g[f"rand_c_op{op}_{tag}"])
+
+
+def test_mlp_oracle_gradient_matches_finite_differences():
+    """The CPU restatement's analytic MLP gradient (the checker of the CUDA
+    backward kernels) agrees with central differences of its own loss."""
+    from oracle import mlp_oracle
+    rng = np.random.default_rng(3)
+    v = 5
+    p = rng.standard_normal(mlp_oracle.param_count(v)) * 0.3
+    x = rng.standard_normal((9, 12))
+    t = rng.standard_normal((9, v))
+    g = mlp_oracle.backward(p, x, t, v)
+    h = 1e-6
+    for i in rng.choice(p.size, 60, replace=False):
+        d = np.zeros_like(p)
+        d[i] = h
+        fd = (mlp_oracle.loss(p + d, x, t, v) - mlp_oracle.loss(p - d, x, t, v)) / (2 * h)
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(g[i]), (i, fd, g[i])
+
+
+def test_feature_oracle_on_a_known_matrix():
+    """Features of a 4 x 4 matrix worked out by hand."""
+    from oracle import mlp_oracle
+    # rows: [0, 1], [], [2, 3, 9?] -> use 16 columns: row 2 has cols 2, 3, 9
+    ptr = np.array([0, 2, 2, 5, 6])
+    idx = np.array([0, 1, 2, 3, 9, 3])
+    f = mlp_oracle.features(4, 16, ptr, idx, 8)
+    assert f[2] == np.log2(7.0)            # nnz = 6
+    assert f[4] == np.log2(4.0)            # longest row 3
+    assert f[6] == 7 / 16                  # |9 - 2| / columns
+    assert f[8] == 3 / 4                   # (0,0), (2,2), (3,3) on the diagonal
+    assert f[9] == 6 / (8 * 4)             # runs: row0 {0,1}, row2 {2,3}, {9}, row3 {3}
+    assert f[10] == 1 / 4 and f[11] == 1.0
