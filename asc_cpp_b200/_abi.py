@@ -80,6 +80,8 @@ class Variant(IntEnum):
 
 
 PLAN_TRANSPOSE = 1
+PLAN_HAS_TRANSPOSE = 1
+PLAN_HAS_BLOCKS16 = 2
 
 
 class SparseDesc(ctypes.Structure):
@@ -154,6 +156,7 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
     "asc_sb_selector_param_count": (ctypes.c_int64, [_I32]),
     "asc_sb_context_set_selector": (ctypes.c_int, [_P, _I32, _P, _P, _P]),
+    "asc_sb_plan_properties": (ctypes.c_int, [_P, ctypes.POINTER(_I32)]),
     "asc_sb_plan_variant": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32)]),
     "asc_sb_plan_autotune": (ctypes.c_int, [_P, _P, _VP, _VP, _I32, _P, _P, _I32, _P]),
     "asc_sb_matrix_features": (ctypes.c_int, [_P, _SP, _P, _P]),

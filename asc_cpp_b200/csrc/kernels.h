@@ -151,6 +151,17 @@ int ascb_complex_spmm(void* stream, int dtype, int mode, int conj, const ascb_cs
                       const void* b, int b_layout, int64_t ldb, void* c, int c_layout,
                       int64_t ldc, double alpha_re, double alpha_im, int sm_count);
 
+// ---- block-sparse SpMM on tensor cores (16 x 16 dense blocks, FP32) ----
+// *bad (device int) becomes 1 unless every block row of `a` (rows a multiple
+// of 16) is made of dense, aligned 16 x 16 blocks.
+int ascb_block16_check(void* stream, const ascb_csr* a, int* bad, int sm_count);
+size_t ascb_block16_tc_smem(void);
+// C += alpha * A * B, row-major B (ldb) and C (ldc); values 16-byte aligned;
+// 3xTF32 on tcgen05.  status (nullable) receives 1 if a bounded wait gave up.
+int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, const float* b,
+                         int64_t ldb, float* c, int64_t ldc, float alpha, int* status,
+                         int sm_count);
+
 // ---- SpMM: C += alpha * op(A) * B (k right-hand sides) ----
 // transpose = 0: stored-order row kernels (exact = 1: the reference's order
 // and rounding; 0: contracted); 1: atomic scatter.

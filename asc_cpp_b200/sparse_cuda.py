@@ -326,6 +326,12 @@ class CsrPlan:
     def handle(self):
         return self._h
 
+    def properties(self) -> int:
+        """Bit set of ASC_SB_PLAN_HAS_TRANSPOSE / ASC_SB_PLAN_HAS_BLOCKS16."""
+        v = ctypes.c_int32()
+        self.context.check(self.context._lib.asc_sb_plan_properties(self._h, ctypes.byref(v)))
+        return v.value
+
     def refresh_values(self) -> None:
         """Re-gathers the transposed values after the matrix's values changed."""
         self.context.check(self.context._lib.asc_sb_plan_refresh_values(

@@ -445,12 +445,16 @@ def run_extra(args):
         flops = 2 * a_h.nnz * k
         bv = sc.DenseMatrixView(B, a_h.cols, k, writable=False)
         cv = sc.DenseMatrixView(C, a_h.rows, k)
+        plan = sc.CsrPlan(ctx, A)  # detects dense 16 x 16 blocks (tensor-core path)
+        extra_cfg["dense_blocks16"] = bool(plan.properties() & 2)
         for name, det in (("deterministic", Determinism.kDeterministic),
                           ("default", Determinism.kBackendDefault)):
             ctx.set_determinism(det)
-            ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv))
+            ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv,
+                                           plan=plan))
             detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
                             "gflops": round(flops / ms / 1e6, 1)}
+        plan.close()
         dtype_s = "f32"
         extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "k": k, "layout": "row-major, ld=k"})
     else:  # batched

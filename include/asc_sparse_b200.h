@@ -275,8 +275,20 @@ ASC_SB_API int asc_sb_plan_standard_spmv(asc_sb_context* context,
                                          double alpha_real, double alpha_imag,
                                          const asc_sb_vector* input,
                                          const asc_sb_vector* output);
+/* What a plan found and holds (bit set): the transposed structure, and
+ * dense, aligned 16 x 16 blocks in an FP32 CSR matrix.  For the latter,
+ * asc_sb_plan_standard_spmm with op = none, row-major B and C, at least 64
+ * right-hand sides, in BACKEND_DEFAULT mode with variant AUTO, runs on the
+ * tensor cores (tcgen05,
+ * FP32 operands split into three TF32 products), within
+ * |c - c_exact| <= (n + 64) 2^-22 |alpha| sum_k |a_k b_k| + 2^-23 |c0| per
+ * output (n = stored entries of the row). */
+enum { ASC_SB_PLAN_HAS_TRANSPOSE = 1, ASC_SB_PLAN_HAS_BLOCKS16 = 2 };
+ASC_SB_API int asc_sb_plan_properties(const asc_sb_plan* plan,
+                                      int32_t* properties);
 /* Standard SpMM through a plan: same contract as asc_sb_standard_spmm, with
- * the transposed products of asc_sb_plan_standard_spmv. */
+ * the transposed products of asc_sb_plan_standard_spmv and the tensor-core
+ * path for dense 16 x 16 blocks above. */
 ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
                                          const asc_sb_plan* plan, int32_t op,
                                          double alpha_real, double alpha_imag,
