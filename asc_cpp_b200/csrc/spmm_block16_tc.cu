@@ -417,17 +417,29 @@ extern "C" int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, 
   using namespace ascb;
   if (a->rows <= 0 || k <= 0) return 0;
   const size_t smem = ascb_block16_tc_smem();
-  const cudaError_t e = cudaFuncSetAttribute(
+  cudaError_t e = cudaFuncSetAttribute(
       block16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+  if (e == cudaSuccess) {
+    // all of the unified L1/shared storage as shared memory: three CTAs fit
+    e = cudaFuncSetAttribute(block16_tc_kernel,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  }
   if (e != cudaSuccess) return static_cast<int>(e);
   const int64_t block_rows = a->rows / 16;
   const int64_t items = block_rows * ((k + kM - 1) / kM);
-  int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, block16_tc_kernel, kThreads,
-                                                    smem) != cudaSuccess ||
-      per_sm < 1) {
+  // CTAs per SM: the shared-memory limit (three at 75 KB each); the register
+  // file (126 x 160 per CTA) allows more
+  int device = 0, sm_smem = 0, reserved = 0;
+  int per_sm = 1;
+  if (cudaGetDevice(&device) == cudaSuccess &&
+      cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) ==
+          cudaSuccess &&
+      cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, device) ==
+          cudaSuccess) {
+    const int fit = sm_smem / static_cast<int>(smem + static_cast<size_t>(reserved));
+    per_sm = fit > 1 ? fit : 1;
+  } else {
     (void)cudaGetLastError();
-    per_sm = 1;
   }
   const int64_t cap = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * per_sm;
   const unsigned grid = static_cast<unsigned>(items < cap ? (items > 0 ? items : 1) : cap);

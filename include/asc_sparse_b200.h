@@ -277,9 +277,8 @@ ASC_SB_API int asc_sb_plan_standard_spmv(asc_sb_context* context,
                                          const asc_sb_vector* output);
 /* What a plan found and holds (bit set): the transposed structure, and
  * dense, aligned 16 x 16 blocks in an FP32 CSR matrix.  For the latter,
- * asc_sb_plan_standard_spmm with op = none, row-major B and C, at least 64
- * right-hand sides, in BACKEND_DEFAULT mode with variant AUTO, runs on the
- * tensor cores (tcgen05,
+ * asc_sb_plan_standard_spmm with op = none, row-major B and C, in
+ * BACKEND_DEFAULT mode with variant AUTO, runs on the tensor cores (tcgen05,
  * FP32 operands split into three TF32 products), within
  * |c - c_exact| <= (n + 64) 2^-22 |alpha| sum_k |a_k b_k| + 2^-23 |c0| per
  * output (n = stored entries of the row). */
