@@ -69,6 +69,18 @@ def _host_threads():
         return os.cpu_count() or 1
 
 
+def max_over_ranks(value: float, world: int, device) -> float:
+    """The largest of every rank's `value` (the job's time is its slowest
+    rank's); every rank must call it, in the same order."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def _matrix(seed=1):
     from asc_cpp_b200 import synthetic
     a = synthetic.power_law(4_194_304, 16.0, 1.5, 65_536, seed=seed, dtype=np.float64)
@@ -262,11 +274,7 @@ def run_gpu(args, rank, world):
         stop.synchronize()
         torch.cuda.synchronize()
         ms = start.elapsed_time(stop) / steps
-        if world > 1:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(ms, world, dev)
 
     # -- variants (untimed selection pass, then the headline) --
     plan = CsrPlan(ctx, A)
