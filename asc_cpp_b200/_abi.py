@@ -122,6 +122,25 @@ class DenseDesc(ctypes.Structure):
                 ("writable", ctypes.c_int32)]
 
 
+class IndexedDesc(ctypes.Structure):
+    _fields_ = [("indices", ctypes.c_void_p),
+                ("values", ctypes.c_void_p),
+                ("memory_space", ctypes.c_int32),
+                ("element_kind", ctypes.c_int32),
+                ("nonzeros", ctypes.c_int64),
+                ("dense_extent", ctypes.c_int64),
+                ("writable", ctypes.c_int32),
+                ("canonical_structure_trusted", ctypes.c_int32)]
+
+
+class Level1Op(IntEnum):
+    kDot = 0
+    kAxpy = 1
+    kGather = 2
+    kGatherZero = 3
+    kScatter = 4
+
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _I64 = ctypes.c_int64
@@ -154,6 +173,8 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
     "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
     "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
+    "asc_sb_standard_level1": (ctypes.c_int, [_P, _I32, _I32, _D, _D,
+                                              ctypes.POINTER(IndexedDesc), _VP, _VP]),
     "asc_sb_selector_param_count": (ctypes.c_int64, [_I32]),
     "asc_sb_context_set_selector": (ctypes.c_int, [_P, _I32, _P, _P, _P]),
     "asc_sb_plan_properties": (ctypes.c_int, [_P, ctypes.POINTER(_I32)]),

@@ -37,12 +37,16 @@ struct asc_sb_context {
   std::string last_error;
   std::atomic<std::int64_t> launches{0};
   int* status = nullptr;  // device word: kernels record bounded-wait timeouts
+  void* scratch = nullptr;  // kContextScratch device bytes after the status word
   // installed variant selector: device parameters and scratch, and the
   // variant (id, lanes) each MLP output stands for
   int selector_outputs = 0;
   float* selector = nullptr;
   std::vector<int> selector_variant, selector_lanes;
 };
+
+constexpr std::size_t kContextScratchOffset = 256;
+constexpr std::size_t kContextScratch = 4096;
 
 // Partitions of one CSR structure, as the kernels consume them.
 struct Partitions {
@@ -494,9 +498,11 @@ int asc_sb_context_create(int32_t device, void* stream, asc_sb_context** out) {
   } else {
     ctx->stream = static_cast<cudaStream_t>(stream);
   }
-  // One device word per context for kernels' bounded-wait timeouts (set-up
-  // allocation; no operation allocates).
-  if (cudaMalloc(reinterpret_cast<void**>(&ctx->status), sizeof(int)) != cudaSuccess ||
+  // One device word per context for kernels' bounded-wait timeouts and a
+  // small scratch (reduction partials) behind it: a set-up allocation, no
+  // operation allocates.
+  if (cudaMalloc(reinterpret_cast<void**>(&ctx->status), kContextScratchOffset + kContextScratch) !=
+          cudaSuccess ||
       cudaMemset(ctx->status, 0, sizeof(int)) != cudaSuccess) {
     (void)cudaGetLastError();
     if (ctx->owns_stream) (void)cudaStreamDestroy(ctx->stream);
@@ -504,6 +510,7 @@ int asc_sb_context_create(int32_t device, void* stream, asc_sb_context** out) {
     delete ctx;
     return ASC_SB_ALLOCATION;
   }
+  ctx->scratch = reinterpret_cast<unsigned char*>(ctx->status) + kContextScratchOffset;
   *out = ctx;
   return ASC_SB_OK;
 }
@@ -1198,6 +1205,117 @@ int asc_sb_convert_coordinates(asc_sb_context* ctx, const int64_t* coordinates,
                    ctx->sm_count),
                "CUDA could not launch the entry permutation kernel");
   return Finish(ctx, s);
+}
+
+// ---------------------------------------------------------------------------
+// Level-1 on an indexed vector.
+
+int asc_sb_standard_level1(asc_sb_context* ctx, int32_t operation, int32_t conjugation,
+                           double alpha_real, double alpha_imag,
+                           const asc_sb_indexed_vector* sparse, const asc_sb_vector* dense,
+                           const asc_sb_vector* result) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (conjugation != ASC_SB_UNCONJUGATED && conjugation != ASC_SB_CONJUGATED) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS conjugation is invalid"));
+  }
+  if (operation < ASC_SB_L1_DOT || operation > ASC_SB_L1_SCATTER) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS level-one operation is invalid"));
+  }
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  if (sparse == nullptr || dense == nullptr ||
+      (operation == ASC_SB_L1_DOT && result == nullptr)) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "level-one descriptors cannot be null"));
+  }
+  // ValidateIndexedDevice (operations.cc:278-332 style rules)
+  const bool sparse_writable =
+      operation == ASC_SB_L1_GATHER || operation == ASC_SB_L1_GATHER_ZERO;
+  if (sparse->memory_space != ASC_SB_DEVICE) {
+    return Finish(ctx, Fail(ASC_SB_MEMORY_ACCESS, "Sparse CUDA indexed vectors require device storage"));
+  }
+  if (sparse->element_kind < ASC_SB_FLOAT || sparse->element_kind > ASC_SB_COMPLEX_DOUBLE) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse CUDA scalar kind is invalid"));
+  }
+  if (!sparse->canonical_structure_trusted) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT,
+                            "Sparse CUDA indexed vectors require trusted canonical structure"));
+  }
+  if (sparse_writable && !sparse->writable) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse CUDA indexed vector is not writable"));
+  }
+  if (sparse->nonzeros < 0 || sparse->dense_extent < 0 ||
+      sparse->nonzeros > sparse->dense_extent) {
+    return Finish(ctx, Fail(ASC_SB_SHAPE, "Sparse CUDA indexed vector extents are invalid"));
+  }
+  const std::size_t element = ascb::host::ElementBytes(sparse->element_kind);
+  const Span idx_span{sparse->indices, static_cast<std::size_t>(sparse->nonzeros) * 8};
+  const Span val_span{sparse->values, static_cast<std::size_t>(sparse->nonzeros) * element};
+  if (sparse->nonzeros > 0) {
+    s = ascb::host::ValidateAddress(sparse->indices, idx_span.bytes, 8,
+                                    "Sparse CUDA index storage is incomplete",
+                                    "Sparse CUDA index storage is misaligned");
+    if (s.ok()) {
+      s = ascb::host::ValidateAddress(sparse->values, val_span.bytes, element > 8 ? 8 : element,
+                                      "Sparse CUDA value storage is incomplete",
+                                      "Sparse CUDA value storage is misaligned");
+    }
+    if (s.ok()) {
+      s = ascb::host::ValidateDevicePointer(sparse->indices, idx_span.bytes, ctx->device,
+                                            "CUDA could not inspect sparse operand storage");
+    }
+    if (s.ok()) {
+      s = ascb::host::ValidateDevicePointer(sparse->values, val_span.bytes, ctx->device,
+                                            "CUDA could not inspect sparse operand storage");
+    }
+    if (!s.ok()) return Finish(ctx, s);
+    if (ascb::host::Overlap(idx_span, val_span)) {
+      return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT,
+                              "Sparse CUDA descriptor storage spans cannot overlap"));
+    }
+  }
+  const bool dense_writable = operation == ASC_SB_L1_AXPY ||
+                              operation == ASC_SB_L1_GATHER_ZERO ||
+                              operation == ASC_SB_L1_SCATTER;
+  Span ds;
+  s = ascb::host::ValidateVector(*dense, sparse->element_kind, dense_writable, ctx->device, &ds);
+  if (!s.ok()) return Finish(ctx, s);
+  if (dense->extent != sparse->dense_extent) {
+    return Finish(ctx, Fail(ASC_SB_SHAPE, "CUDA Sparse BLAS level-one vector extents do not match"));
+  }
+  if (operation != ASC_SB_L1_DOT &&
+      (ascb::host::Overlap(val_span, ds) || ascb::host::Overlap(idx_span, ds))) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT,
+                            "CUDA Sparse BLAS level-one writable operands overlap"));
+  }
+  Span rs;
+  if (operation == ASC_SB_L1_DOT) {
+    s = ascb::host::ValidateVector(*result, sparse->element_kind, true, ctx->device, &rs);
+    if (!s.ok()) return Finish(ctx, s);
+    if (result->extent != 1) {
+      return Finish(ctx, Fail(ASC_SB_SHAPE, "CUDA sparse dot requires one result element"));
+    }
+    if (ascb::host::Overlap(rs, ds) || ascb::host::Overlap(rs, idx_span) ||
+        ascb::host::Overlap(rs, val_span)) {
+      return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "CUDA sparse dot result overlaps an input"));
+    }
+  }
+  if (operation == ASC_SB_L1_AXPY &&
+      AlphaIsZero(sparse->element_kind, alpha_real, alpha_imag)) {
+    return Finish(ctx, Status::Ok());
+  }
+  if (operation != ASC_SB_L1_DOT && sparse->nonzeros == 0) return Finish(ctx, Status::Ok());
+  return Finish(ctx, Launched(ctx,
+                              ascb_level1(ctx->stream, Dtype(sparse->element_kind), operation,
+                                          conjugation, ctx->determinism == ASC_SB_DETERMINISTIC,
+                                          static_cast<const std::int64_t*>(sparse->indices),
+                                          const_cast<void*>(sparse->values), sparse->nonzeros,
+                                          const_cast<void*>(dense->data), dense->stride,
+                                          result != nullptr ? const_cast<void*>(result->data)
+                                                            : nullptr,
+                                          alpha_real, alpha_imag, ctx->scratch, ctx->sm_count),
+                              "CUDA could not launch the level-one kernel"));
 }
 
 // ---------------------------------------------------------------------------

@@ -162,6 +162,17 @@ int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, const float
                          int64_t ldb, float* c, int64_t ldc, float alpha, int* status,
                          int sm_count);
 
+// ---- Level-1 on an indexed vector (internal_sparse_cuda::StandardOperation) ----
+enum { ASCB_L1_DOT = 0, ASCB_L1_AXPY = 1, ASCB_L1_GATHER = 2, ASCB_L1_GATHER_ZERO = 3,
+       ASCB_L1_SCATTER = 4 };
+#define ASCB_L1_DOT_BLOCKS 256
+// idx/val: n entries; x: dense vector (logical element 0, stride incx);
+// result: one element (dot).  exact = 1: the reference's order and rounding
+// for the dot.  scratch: ASCB_L1_DOT_BLOCKS elements for the contracted dot.
+int ascb_level1(void* stream, int dtype, int op, int conj, int exact, const int64_t* idx,
+                void* val, int64_t n, void* x, int64_t incx, void* result, double alpha_re,
+                double alpha_im, void* scratch, int sm_count);
+
 // ---- SpMM: C += alpha * op(A) * B (k right-hand sides) ----
 // transpose = 0: stored-order row kernels (exact = 1: the reference's order
 // and rounding; 0: contracted); 1: atomic scatter.

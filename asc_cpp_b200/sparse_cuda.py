@@ -484,3 +484,34 @@ class CudaBatch:
             self.close()
         except Exception:
             pass
+
+
+# ---- Level-1 on an indexed vector (blas.h:1340-1600 semantics) ----
+
+def CudaLevel1(context: SparseCudaContext, operation: int, indices: torch.Tensor,
+               values: torch.Tensor, dense: CudaStridedVectorView,
+               result: torch.Tensor | None = None, alpha: complex = 0.0,
+               conjugated: bool = False) -> None:
+    """dot (result[0]), axpy, gather, gather-zero or scatter between the
+    indexed vector (indices, values) and `dense` (internal_sparse_cuda::
+    StandardLevel1Erased)."""
+    from ._abi import IndexedDesc, Level1Op
+    op = int(operation)
+    d = IndexedDesc()
+    d.indices = indices.data_ptr() if indices.numel() else None
+    d.values = values.data_ptr() if values.numel() else None
+    d.memory_space = MemorySpace.kDevice
+    d.element_kind = _kind(values.dtype)
+    d.nonzeros = int(values.numel())
+    d.dense_extent = dense.extent
+    d.writable = 1 if op in (Level1Op.kGather, Level1Op.kGatherZero) else 0
+    d.canonical_structure_trusted = 1
+    dd = dense.describe()
+    dd.writable = 1 if op in (Level1Op.kAxpy, Level1Op.kGatherZero, Level1Op.kScatter) else 0
+    rd = None
+    if op == Level1Op.kDot:
+        rd = CudaStridedVectorView(result, 1).describe()
+    a = complex(alpha)
+    context.check(context._lib.asc_sb_standard_level1(
+        context.handle, op, 1 if conjugated else 0, a.real, a.imag, ctypes.byref(d),
+        ctypes.byref(dd), ctypes.byref(rd) if rd is not None else None))

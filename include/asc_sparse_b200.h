@@ -242,6 +242,45 @@ ASC_SB_API int asc_sb_standard_spmm(asc_sb_context* context, int32_t op,
                                     const asc_sb_dense* input,
                                     const asc_sb_dense* output);
 
+/* ---- Level-1 on an indexed vector ------------------------------------------ */
+
+/* internal_sparse_cuda::IndexedVectorDescriptor, cuda.h:175-184: int64
+ * indices [nonzeros] (sorted, unique, below dense_extent; the caller asserts
+ * it with canonical_structure_trusted) and values [nonzeros]. */
+typedef struct asc_sb_indexed_vector {
+  const void* indices;
+  const void* values;
+  int32_t memory_space;
+  int32_t element_kind;
+  int64_t nonzeros;
+  int64_t dense_extent;
+  int32_t writable;
+  int32_t canonical_structure_trusted;
+} asc_sb_indexed_vector;
+
+/* internal_sparse_cuda::StandardOperation, cuda.h:111-117 */
+enum { ASC_SB_L1_DOT = 0, ASC_SB_L1_AXPY = 1, ASC_SB_L1_GATHER = 2,
+       ASC_SB_L1_GATHER_ZERO = 3, ASC_SB_L1_SCATTER = 4 };
+/* asc::SparseBlasConjugation, blas.h:74-77 */
+enum { ASC_SB_UNCONJUGATED = 0, ASC_SB_CONJUGATED = 1 };
+
+/* Replaces internal_sparse_cuda::StandardLevel1Erased (cuda.h:228-233;
+ * operations.cc:1122-1212), CPU contract blas.h:1340-1600:
+ *   DOT          result[0] = sum_k v'_k x[i_k]  (v' = conj(v) if CONJUGATED)
+ *   AXPY         x[i_k] += alpha v_k   (alpha == 0: nothing is touched)
+ *   GATHER       v_k = x[i_k]
+ *   GATHER_ZERO  v_k = x[i_k]; x[i_k] = 0
+ *   SCATTER      x[i_k] = v_k
+ * All four element kinds.  The element-wise operations are exact; the dot in
+ * DETERMINISTIC mode adds in stored order with the reference's rounding (bit
+ * for bit), in BACKEND_DEFAULT mode with a fixed reduction tree. */
+ASC_SB_API int asc_sb_standard_level1(asc_sb_context* context, int32_t operation,
+                                      int32_t conjugation, double alpha_real,
+                                      double alpha_imag,
+                                      const asc_sb_indexed_vector* sparse,
+                                      const asc_sb_vector* dense,
+                                      const asc_sb_vector* result);
+
 /* ---- analysis plans (no reference counterpart) ----------------------------
  * A plan caches, in caller-provided device memory, everything the kernels can
  * reuse across calls on one matrix: the row-tile and merge-path partitions and

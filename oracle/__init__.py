@@ -94,6 +94,14 @@ class Restatement:
             f.restype = None
             f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, sc, sc, _P, _INT,
                           _I64, _P, _INT, _I64, _I64]
+        for sfx, sc in (("f64", ctypes.c_double), ("f32", ctypes.c_float)):
+            f = getattr(self.lib, f"oracle_level1_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _INT, _P, _P, _I64, sc, _P, _P]
+        for sfx, sc in (("z", ctypes.c_double), ("c", ctypes.c_float)):
+            f = getattr(self.lib, f"oracle_level1_{sfx}")
+            f.restype = None
+            f.argtypes = [_INT, _INT, _P, _P, _I64, sc, sc, _P, _P]
         self.lib.oracle_output_counts.restype = None
         self.lib.oracle_output_counts.argtypes = [_INT, _I64, _I64, _P, _P, _P]
         self.lib.oracle_csr_transpose_structure.restype = None
@@ -177,6 +185,25 @@ class Restatement:
                                                 _ptr(t_idx), _ptr(perm))
         return t_ptr, t_idx[:nnz], perm[:nnz]
 
+    def level1(self, op, conj, idx, val, alpha, x):
+        """Level-1 on copies: returns (values, dense, dot result)."""
+        val = val.copy()
+        x = x.copy()
+        res = np.zeros(1, dtype=val.dtype)
+        idx = np.ascontiguousarray(idx, np.int64)
+        cs = _complex_suffix(val.dtype)
+        if cs is not None:
+            rs = _real_scalar(val.dtype)
+            a = complex(alpha)
+            getattr(self.lib, f"oracle_level1_{cs}")(op, conj, _ptr(idx), _ptr(val), len(idx),
+                                                     rs(a.real), rs(a.imag), _ptr(x), _ptr(res))
+        else:
+            sc = _scalar(val.dtype)
+            getattr(self.lib, f"oracle_level1_{_suffix(val.dtype)}")(
+                op, conj, _ptr(idx), _ptr(val), len(idx), sc(float(np.real(alpha))), _ptr(x),
+                _ptr(res))
+        return val, x, res[0]
+
     def stable_bucket_sort(self, keys, kstride, n, limit):
         """(offsets[limit+1], perm[n]) of the stable sort of keys[e*kstride]."""
         offsets = np.zeros(limit + 1, dtype=np.int64)
@@ -256,6 +283,11 @@ class Reference:
             f.argtypes = [_INT, _INT, _I64, _I64, _P, _P, _P, _I64, sc, sc, _P,
                           _I64, _I64, _INT, _I64, _SZ, _P, _I64, _I64, _INT,
                           _I64, _SZ]
+        for sfx, sc in (("f64", ctypes.c_double), ("f32", ctypes.c_float),
+                        ("z", ctypes.c_double), ("c", ctypes.c_float)):
+            f = getattr(self.lib, f"ref_level1_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _P, _P, _I64, _I64, sc, sc, _P, _P]
         f = self.lib.ref_convert_compressed_f64
         f.restype = _INT
         f.argtypes = [_INT, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P]
@@ -359,3 +391,19 @@ class Reference:
         if rc != 0:
             raise RuntimeError(f"reference conversion failed with code {rc}")
         return o, i[:nnz], v[:nnz]
+
+    def level1(self, op, conj, idx, val, alpha, x):
+        """The reference's Level-1 on copies: (values, dense, dot result)."""
+        val = val.copy()
+        x = x.copy()
+        res = np.zeros(1, dtype=val.dtype)
+        idx = np.ascontiguousarray(idx, np.int64)
+        sfx = _complex_suffix(val.dtype) or _suffix(val.dtype)
+        rs = _real_scalar(val.dtype) if _complex_suffix(val.dtype) else _scalar(val.dtype)
+        a = complex(alpha)
+        rc = getattr(self.lib, f"ref_level1_{sfx}")(op, conj, _ptr(idx), _ptr(val), len(idx),
+                                                    x.size, rs(a.real), rs(a.imag), _ptr(x),
+                                                    _ptr(res))
+        if rc != 0:
+            raise RuntimeError(f"reference level-one failed with code {rc}")
+        return val, x, res[0]

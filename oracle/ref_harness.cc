@@ -327,6 +327,65 @@ int ConvertCoordinates(int to_csc, std::int64_t rows, std::int64_t cols,
   return CopyOut(*dst, rows, out_ptr, out_idx, out_val);
 }
 
+template <typename T, typename R>
+T MakeScalar(R re, R im) {
+  if constexpr (sizeof(T) == 2 * sizeof(R)) {
+    return T(re, im);
+  } else {
+    (void)im;
+    return T(re);
+  }
+}
+
+// Level-1 on an indexed vector through the reference's SparseDot /
+// SparseAxpy / SparseGather / SparseGatherZero / SparseScatter
+// (blas.h:1340-1600).  op: 0 dot, 1 axpy, 2 gather, 3 gather-zero,
+// 4 scatter; x is the dense vector (unit stride), result receives the dot.
+template <typename T>
+int Level1(int op, int conj, const std::int64_t* idx, T* val, std::int64_t nnz,
+           std::int64_t n, T alpha, T* x, T* result) {
+  const asc::ConstMemoryView idx_storage{idx, static_cast<std::size_t>(nnz) * 8,
+                                         asc::MemorySpace::kHost};
+  const asc::ConstMemoryView val_storage{val, static_cast<std::size_t>(nnz) * sizeof(T),
+                                         asc::MemorySpace::kHost};
+  const asc::ConstMemoryView x_const{x, static_cast<std::size_t>(n) * sizeof(T),
+                                     asc::MemorySpace::kHost};
+  const asc::MutableMemoryView x_mut{x, static_cast<std::size_t>(n) * sizeof(T),
+                                     asc::MemorySpace::kHost};
+  const auto context = asc::ExecutionContext::Serial();
+  if (op == 0 || op == 1 || op == 4) {
+    auto sparse = asc::SparseBlasIndexedVectorView<const T>::Create(idx, val, nnz, n, idx_storage,
+                                                                    val_storage);
+    if (!sparse.ok()) return Code(sparse.status());
+    if (op == 0) {
+      auto dense = asc::SparseBlasVectorView<const T>::Create(x, n, 1, x_const);
+      if (!dense.ok()) return Code(dense.status());
+      auto r = asc::SparseDot(context,
+                              conj ? asc::SparseBlasConjugation::kConjugated
+                                   : asc::SparseBlasConjugation::kUnconjugated,
+                              *sparse, *dense);
+      if (!r.ok()) return Code(r.status());
+      *result = *r;
+      return 0;
+    }
+    auto dense = asc::SparseBlasVectorView<T>::Create(x, n, 1, x_mut);
+    if (!dense.ok()) return Code(dense.status());
+    return op == 1 ? Code(asc::SparseAxpy(context, alpha, *sparse, *dense))
+                   : Code(asc::SparseScatter(context, *sparse, *dense));
+  }
+  auto sparse = asc::SparseBlasIndexedVectorView<T>::Create(idx, val, nnz, n, idx_storage,
+                                                            val_storage);
+  if (!sparse.ok()) return Code(sparse.status());
+  if (op == 2) {
+    auto dense = asc::SparseBlasVectorView<const T>::Create(x, n, 1, x_const);
+    if (!dense.ok()) return Code(dense.status());
+    return Code(asc::SparseGather(context, *dense, *sparse));
+  }
+  auto dense = asc::SparseBlasVectorView<T>::Create(x, n, 1, x_mut);
+  if (!dense.ok()) return Code(dense.status());
+  return Code(asc::SparseGatherZero(context, *dense, *sparse));
+}
+
 }  // namespace
 
 extern "C" {
@@ -478,5 +537,19 @@ int ref_convert_coordinates_f64(int to_csc, std::int64_t rows,
   return ConvertCoordinates<double>(to_csc, rows, cols, coordinates, val, nnz,
                                     out_ptr, out_idx, out_val);
 }
+
+#define ASC_REF_LEVEL1(SUFFIX, T, R)                                            \
+  int ref_level1_##SUFFIX(int op, int conj, const std::int64_t* idx, R* val,    \
+                          std::int64_t nnz, std::int64_t n, R alpha_re,         \
+                          R alpha_im, R* x, R* result) {                        \
+    const T alpha = MakeScalar<T>(alpha_re, alpha_im);                          \
+    return Level1<T>(op, conj, idx, reinterpret_cast<T*>(val), nnz, n, alpha,   \
+                     reinterpret_cast<T*>(x), reinterpret_cast<T*>(result));    \
+  }
+ASC_REF_LEVEL1(f64, double, double)
+ASC_REF_LEVEL1(f32, float, float)
+ASC_REF_LEVEL1(z, std::complex<double>, double)
+ASC_REF_LEVEL1(c, std::complex<float>, float)
+#undef ASC_REF_LEVEL1
 
 }  // extern "C"

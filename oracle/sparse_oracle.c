@@ -205,6 +205,69 @@ ORACLE_COMPLEX(z, double)
 ORACLE_COMPLEX(c, float)
 
 /* ------------------------------------------------------------------------- */
+/* Level-1 on an indexed vector (blas.h:1340-1600): op 0 dot (serial, from
+ * zero, result += v' * x[i]), 1 axpy (x[i] += alpha * v), 2 gather, 3
+ * gather-zero, 4 scatter.  Complex variants work on (re, im) pairs with the
+ * products of ORACLE_COMPLEX above.                                        */
+#define ORACLE_LEVEL1(SUFFIX, T)                                               \
+  void oracle_level1_##SUFFIX(int op, int conj, const int64_t* idx, T* val,    \
+                              int64_t nnz, T alpha, T* x, T* result) {         \
+    (void)conj;                                                                \
+    if (op == 0) {                                                             \
+      T sum = (T)0;                                                            \
+      for (int64_t q = 0; q < nnz; ++q) sum += val[q] * x[idx[q]];             \
+      *result = sum;                                                           \
+      return;                                                                  \
+    }                                                                          \
+    if (op == 1 && alpha == (T)0) return;                                      \
+    for (int64_t q = 0; q < nnz; ++q) {                                        \
+      T* xi = &x[idx[q]];                                                      \
+      if (op == 1) *xi += alpha * val[q];                                      \
+      if (op == 2) val[q] = *xi;                                               \
+      if (op == 3) { val[q] = *xi; *xi = (T)0; }                               \
+      if (op == 4) *xi = val[q];                                               \
+    }                                                                          \
+  }
+ORACLE_LEVEL1(f64, double)
+ORACLE_LEVEL1(f32, float)
+
+#define ORACLE_LEVEL1_COMPLEX(SUFFIX, T)                                       \
+  void oracle_level1_##SUFFIX(int op, int conj, const int64_t* idx, T* val,    \
+                              int64_t nnz, T al_r, T al_i, T* x, T* result) {  \
+    if (op == 0) {                                                             \
+      T sr = (T)0, si = (T)0;                                                  \
+      for (int64_t q = 0; q < nnz; ++q) {                                      \
+        T pr, pi;                                                              \
+        const T vi = conj ? -val[2 * q + 1] : val[2 * q + 1];                  \
+        cmul_##SUFFIX(val[2 * q], vi, x[2 * idx[q]], x[2 * idx[q] + 1], &pr,   \
+                      &pi);                                                    \
+        sr += pr;                                                              \
+        si += pi;                                                              \
+      }                                                                        \
+      result[0] = sr;                                                          \
+      result[1] = si;                                                          \
+      return;                                                                  \
+    }                                                                          \
+    if (op == 1 && al_r == (T)0 && al_i == (T)0) return;                       \
+    for (int64_t q = 0; q < nnz; ++q) {                                        \
+      T* xi = &x[2 * idx[q]];                                                  \
+      if (op == 1) {                                                           \
+        T pr, pi;                                                              \
+        cmul_##SUFFIX(al_r, al_i, val[2 * q], val[2 * q + 1], &pr, &pi);       \
+        xi[0] += pr;                                                           \
+        xi[1] += pi;                                                           \
+      }                                                                        \
+      if (op == 2) { val[2 * q] = xi[0]; val[2 * q + 1] = xi[1]; }             \
+      if (op == 3) {                                                           \
+        val[2 * q] = xi[0]; val[2 * q + 1] = xi[1]; xi[0] = (T)0; xi[1] = (T)0; \
+      }                                                                        \
+      if (op == 4) { xi[0] = val[2 * q]; xi[1] = val[2 * q + 1]; }             \
+    }                                                                          \
+  }
+ORACLE_LEVEL1_COMPLEX(z, double)
+ORACLE_LEVEL1_COMPLEX(c, float)
+
+/* ------------------------------------------------------------------------- */
 /* Extended-precision companions used to state and check error bounds.
  * For each output o of op(A) (CSR, unit-stride vectors) they return
  *   exact[o] ~= sum_k v_k x_k   (long double accumulation of exact products)

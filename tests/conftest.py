@@ -37,6 +37,11 @@ def known_answers():
 
 
 @pytest.fixture(scope="session")
+def level1_cases():
+    return dict(np.load(os.path.join(GOLDEN, "level1_cases.npz")))
+
+
+@pytest.fixture(scope="session")
 def complex_cases():
     return dict(np.load(os.path.join(GOLDEN, "complex_cases.npz")))
 

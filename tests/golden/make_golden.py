@@ -32,6 +32,10 @@ into oracle/_ref/libasc_ref.so by oracle/build_oracle.py).  The fixtures pin:
   tests/sparse/standard_blas_test.cc:177-345 (CSR none, conjugate transpose,
   CSC none; row-major SpMM, column-major conjugate-transposed CSC SpMM) and a
   seeded random 300 x 220 matrix for every op.
+* ``level1_cases.npz`` - the reference's dot (plain and conjugated), axpy,
+  gather, gather-zero and scatter on the indexed vector of
+  tests/sparse/standard_blas_test.cc:69-173 and on a seeded random one, for
+  FP64, FP32, Z and C.
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -273,6 +277,34 @@ def complex_cases(ref: Reference) -> dict[str, np.ndarray]:
     return out
 
 
+def level1_cases(ref: Reference) -> dict[str, np.ndarray]:
+    """The reference's Level-1 operations (blas.h:1340-1600) on the values of
+    standard_blas_test.cc:69-173 (indices {0, 2}, dense length 3) and on a
+    seeded random indexed vector, for all four element kinds and every op."""
+    out: dict[str, np.ndarray] = {}
+    rng = np.random.default_rng(61)
+    for dt, tag in ((np.float64, "f64"), (np.float32, "f32"), (np.complex128, "z"),
+                    (np.complex64, "c")):
+        cplx = np.iscomplexobj(dt(0))
+        ka_idx = np.array([0, 2], np.int64)
+        ka_val = np.array([1 + 2j, -2 + 1j] if cplx else [1.0, -2.0], dt)
+        ka_x = np.array([3 - 1j, 9 + 4j, 2 + 3j] if cplx else [3.0, 9.0, 2.0], dt)
+        n = 4000
+        r_idx = np.sort(rng.choice(n, 1500, replace=False)).astype(np.int64)
+        r_val = (rng.standard_normal(1500) + (1j * rng.standard_normal(1500) if cplx else 0)).astype(dt)
+        r_x = (rng.standard_normal(n) + (1j * rng.standard_normal(n) if cplx else 0)).astype(dt)
+        alpha = (0.75 - 1.5j) if cplx else 2.0
+        for name, (idx, val, x) in (("ka", (ka_idx, ka_val, ka_x)), ("rand", (r_idx, r_val, r_x))):
+            out[f"{name}_idx_{tag}"], out[f"{name}_val_{tag}"], out[f"{name}_x_{tag}"] = idx, val, x
+            for op in range(5):
+                for conj in ((0, 1) if op == 0 else (0,)):
+                    v, xx, r = ref.level1(op, conj, idx, val, alpha, x)
+                    key = f"{name}_op{op}_conj{conj}_{tag}"
+                    out[key + "_val"], out[key + "_x"] = v, xx
+                    out[key + "_res"] = np.array([r], dt)
+    return out
+
+
 def main() -> None:
     build_oracle.build_reference()
     ref = Reference()
@@ -281,8 +313,9 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "laplacian.npz"), **laplacian(ref))
     np.savez_compressed(os.path.join(HERE, "conversions.npz"), **conversions(ref))
     np.savez_compressed(os.path.join(HERE, "complex_cases.npz"), **complex_cases(ref))
+    np.savez_compressed(os.path.join(HERE, "level1_cases.npz"), **level1_cases(ref))
     for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz", "conversions.npz",
-              "complex_cases.npz"):
+              "complex_cases.npz", "level1_cases.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))
 
 

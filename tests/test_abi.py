@@ -62,9 +62,10 @@ def test_descriptor_layouts_match_header():
 #include <stdio.h>
 #include "asc_sparse_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(asc_sb_sparse), sizeof(asc_sb_vector),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(asc_sb_sparse), sizeof(asc_sb_vector),
          sizeof(asc_sb_dense), offsetof(asc_sb_sparse, rows), offsetof(asc_sb_vector, extent),
-         offsetof(asc_sb_dense, leading_dimension), offsetof(asc_sb_dense, writable));
+         offsetof(asc_sb_dense, leading_dimension), offsetof(asc_sb_dense, writable),
+         sizeof(asc_sb_indexed_vector), offsetof(asc_sb_indexed_vector, dense_extent));
   return 0;
 }
 '''
@@ -79,7 +80,8 @@ int main(void) {
     want = [ctypes.sizeof(_abi.SparseDesc), ctypes.sizeof(_abi.VectorDesc),
             ctypes.sizeof(_abi.DenseDesc), _abi.SparseDesc.rows.offset,
             _abi.VectorDesc.extent.offset, _abi.DenseDesc.leading_dimension.offset,
-            _abi.DenseDesc.writable.offset]
+            _abi.DenseDesc.writable.offset, ctypes.sizeof(_abi.IndexedDesc),
+            _abi.IndexedDesc.dense_extent.offset]
     assert got == want
 
 

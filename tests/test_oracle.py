@@ -287,3 +287,28 @@ def test_feature_oracle_on_a_known_matrix():
     assert f[8] == 3 / 4                   # (0,0), (2,2), (3,3) on the diagonal
     assert f[9] == 6 / (8 * 4)             # runs: row0 {0,1}, row2 {2,3}, {9}, row3 {3}
     assert f[10] == 1 / 4 and f[11] == 1.0
+
+
+@pytest.mark.parametrize("tag", ["f64", "f32", "z", "c"])
+def test_level1_restatement_matches_reference_fixtures(restatement, level1_cases, tag):
+    """Dot, axpy, gather, gather-zero and scatter of the oracle equal the
+    reference's on standard_blas_test.cc:69-173 and a random case."""
+    g = level1_cases
+    for name in ("ka", "rand"):
+        idx, val, x = g[f"{name}_idx_{tag}"], g[f"{name}_val_{tag}"], g[f"{name}_x_{tag}"]
+        alpha = (0.75 - 1.5j) if np.iscomplexobj(val) else 2.0
+        for op in range(5):
+            for conj in ((0, 1) if op == 0 else (0,)):
+                v, xx, r = restatement.level1(op, conj, idx, val, alpha, x)
+                key = f"{name}_op{op}_conj{conj}_{tag}"
+                assert _bits_equal(v, g[key + "_val"]) and _bits_equal(xx, g[key + "_x"])
+                if op == 0:
+                    assert _bits_equal(np.array([r], val.dtype), g[key + "_res"])
+
+
+def test_level1_known_answer_values(level1_cases):
+    """standard_blas_test.cc:69-173 expectations, literally: the dot of
+    {1, -2} at {0, 2} with {3, 9, 2} is -1; axpy with alpha 2 gives {5, 9, -2}."""
+    assert level1_cases["ka_op0_conj0_f64_res"][0] == -1.0
+    assert level1_cases["ka_op1_conj0_f64_x"].tolist() == [5.0, 9.0, -2.0]
+    assert level1_cases["ka_op3_conj0_f64_x"].tolist() == [0.0, 9.0, 0.0]
