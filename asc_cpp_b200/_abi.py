@@ -80,6 +80,7 @@ class Variant(IntEnum):
 
 
 PLAN_TRANSPOSE = 1
+PLAN_TRIANGULAR = 2
 PLAN_HAS_TRANSPOSE = 1
 PLAN_HAS_BLOCKS16 = 2
 
@@ -133,6 +134,18 @@ class IndexedDesc(ctypes.Structure):
                 ("canonical_structure_trusted", ctypes.c_int32)]
 
 
+class SparseBlasTriangle(IntEnum):
+    """asc::SparseBlasTriangle (include/asc/sparse/blas.h:117-120)."""
+    kUpper = 0
+    kLower = 1
+
+
+class SparseBlasDiagonal(IntEnum):
+    """asc::SparseBlasDiagonal (include/asc/sparse/blas.h:131-134)."""
+    kNonUnit = 0
+    kUnit = 1
+
+
 class Level1Op(IntEnum):
     kDot = 0
     kAxpy = 1
@@ -173,6 +186,9 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
     "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
     "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
+    "asc_sb_standard_triangular_solve": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _I32, _I32,
+                                                        _DP]),
+    "asc_sb_plan_triangular_solve": (ctypes.c_int, [_P, _P, _I32, _D, _D, _I32, _I32, _DP]),
     "asc_sb_standard_level1": (ctypes.c_int, [_P, _I32, _I32, _D, _D,
                                               ctypes.POINTER(IndexedDesc), _VP, _VP]),
     "asc_sb_selector_param_count": (ctypes.c_int64, [_I32]),

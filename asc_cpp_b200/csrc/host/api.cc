@@ -43,6 +43,11 @@ struct asc_sb_context {
   int selector_outputs = 0;
   float* selector = nullptr;
   std::vector<int> selector_variant, selector_lanes;
+  // triangular solves without a plan: ready flags (and, for transposed
+  // solves, the transposed structure) in a buffer that grows to the largest
+  // solve seen
+  void* solve_scratch = nullptr;
+  std::size_t solve_bytes = 0;
 };
 
 constexpr std::size_t kContextScratchOffset = 256;
@@ -73,6 +78,8 @@ struct asc_sb_plan {
   // FP32 CSR made of dense, aligned 16 x 16 blocks: SpMM runs on the tensor
   // cores in BACKEND_DEFAULT mode
   bool block16 = false;
+  // ASC_SB_PLAN_TRIANGULAR: control block and ready flags of the solves
+  unsigned char* solve = nullptr;
 };
 
 namespace {
@@ -309,7 +316,7 @@ std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
 struct PlanLayout {
   std::size_t flag = 0;  // one device int for structure checks
   std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, t_part = 0;
-  std::size_t sort = 0, outer_of = 0, total = 0;
+  std::size_t sort = 0, outer_of = 0, solve = 0, total = 0;
 };
 
 PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
@@ -336,6 +343,10 @@ PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
     at += RoundUp(ascb_sort_workspace_bytes(nnz, inner), 256);
     l.outer_of = at;
     at += EntryBytes(nnz, 8);
+  }
+  if (flags & ASC_SB_PLAN_TRIANGULAR) {
+    l.solve = at;
+    at += RoundUp(ascb_trsv_scratch_bytes(outer), 256);
   }
   l.total = at;
   return l;
@@ -522,6 +533,7 @@ int asc_sb_context_destroy(asc_sb_context* ctx) {
   if (ctx->owns_stream) (void)cudaStreamDestroy(ctx->stream);
   if (ctx->status != nullptr) (void)cudaFree(ctx->status);
   if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
+  if (ctx->solve_scratch != nullptr) (void)cudaFree(ctx->solve_scratch);
   delete ctx;
   return ASC_SB_OK;
 }
@@ -879,7 +891,7 @@ int asc_sb_plan_workspace_size(asc_sb_context* ctx, const asc_sb_sparse* m, int3
   if (m == nullptr || bytes == nullptr) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "plan arguments cannot be null"));
   }
-  if ((flags & ~ASC_SB_PLAN_TRANSPOSE) != 0) {
+  if ((flags & ~(ASC_SB_PLAN_TRANSPOSE | ASC_SB_PLAN_TRIANGULAR)) != 0) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "unknown plan flags"));
   }
   if (m->rows < 0 || m->columns < 0 || m->nonzeros < 0) {
@@ -930,6 +942,7 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
                         reinterpret_cast<std::int64_t*>(ws + l.outer_of));
     if (s.ok()) s = BuildPartitions(ctx, TransposedCsr(*plan), ws + l.t_part, &plan->t_part);
   }
+  if (flags & ASC_SB_PLAN_TRIANGULAR) plan->solve = ws + PlanLayoutFor(*m, flags).solve;
   if (s.ok() && m->format == ASC_SB_CSR && m->element_kind == ASC_SB_FLOAT && m->rows > 0 &&
       m->rows % 16 == 0 && m->nonzeros > 0 &&
       (reinterpret_cast<std::uintptr_t>(m->values) & 15u) == 0) {
@@ -1316,6 +1329,170 @@ int asc_sb_standard_level1(asc_sb_context* ctx, int32_t operation, int32_t conju
                                                             : nullptr,
                                           alpha_real, alpha_imag, ctx->scratch, ctx->sm_count),
                               "CUDA could not launch the level-one kernel"));
+}
+
+// ---------------------------------------------------------------------------
+// Sparse triangular solve.
+
+namespace {
+
+// Grows the context's solve buffer to `bytes`.  A larger buffer replaces the
+// old one only after the stream has finished with it.
+Status SolveScratch(asc_sb_context* ctx, std::size_t bytes, unsigned char** out) {
+  if (ctx->solve_bytes < bytes) {
+    if (ctx->solve_scratch != nullptr) {
+      if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return Fail(ASC_SB_PROVIDER, "CUDA could not drain the stream before growing scratch");
+      }
+      (void)cudaFree(ctx->solve_scratch);
+      ctx->solve_scratch = nullptr;
+      ctx->solve_bytes = 0;
+    }
+    if (cudaMalloc(&ctx->solve_scratch, bytes) != cudaSuccess) {
+      (void)cudaGetLastError();
+      ctx->solve_scratch = nullptr;
+      return Fail(ASC_SB_ALLOCATION, "CUDA could not allocate triangular-solve scratch");
+    }
+    ctx->solve_bytes = bytes;
+  }
+  *out = static_cast<unsigned char*>(ctx->solve_scratch);
+  return Status::Ok();
+}
+
+// StandardTriangularSolveErased (operations.cc:1380-1451): validation in the
+// facet's order, then one sync-free solve on the CSR arrays of op(A).
+Status TriangularSolve(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double alpha_real,
+                       double alpha_imag, const asc_sb_sparse* m, int triangle, int diagonal,
+                       const asc_sb_dense* rhs) {
+  if (op != ASC_SB_OP_NONE && op != ASC_SB_OP_TRANSPOSE && op != ASC_SB_OP_CONJUGATE_TRANSPOSE) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS transpose mode is invalid");
+  }
+  if (triangle != ASC_SB_UPPER && triangle != ASC_SB_LOWER) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "A sparse BLAS triangle value is invalid");
+  }
+  if (diagonal != ASC_SB_NON_UNIT && diagonal != ASC_SB_UNIT) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "A sparse BLAS diagonal value is invalid");
+  }
+  if (m == nullptr || rhs == nullptr) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "CUDA triangular-solve descriptors cannot be null");
+  }
+  if (m->format != ASC_SB_CSR || m->rows != m->columns) {
+    return Fail(ASC_SB_SHAPE, "CUDA triangular solve requires square CSR storage");
+  }
+  SparseBytes mb;
+  Status s = ascb::host::ValidateSparse(*m, ctx->device, &mb);
+  if (!s.ok()) return s;
+  Span rs;
+  s = ascb::host::ValidateDense(*rhs, m->element_kind, true, ctx->device, &rs);
+  if (!s.ok()) return s;
+  if (rhs->rows != m->rows) {
+    return Fail(ASC_SB_SHAPE, "CUDA triangular right-hand-side extent does not match");
+  }
+  if (ascb::host::Overlap({m->structure_first, mb.first}, rs) ||
+      ascb::host::Overlap({m->structure_second, mb.second}, rs) ||
+      ascb::host::Overlap({m->values, mb.values}, rs)) {
+    return Fail(ASC_SB_INVALID_ARGUMENT, "CUDA triangular right-hand sides overlap the matrix");
+  }
+  const std::int64_t n = m->rows;
+  const bool transposed = op != ASC_SB_OP_NONE;
+  if (plan != nullptr) {
+    if (plan->solve == nullptr) {
+      return Fail(ASC_SB_INVALID_STATE, "the plan holds no triangular-solve state");
+    }
+    if (transposed && plan->t_ptr == nullptr) {
+      return Fail(ASC_SB_INVALID_STATE, "a transposed solve needs a plan with the transposed structure");
+    }
+  }
+  if (n == 0 || rhs->columns == 0) return Status::Ok();
+  const bool alpha_zero = AlphaIsZero(m->element_kind, alpha_real, alpha_imag);
+  ascb_csr op_csr = AsCsr(*m, false);
+  unsigned char* control = nullptr;
+  if (plan != nullptr) {
+    control = plan->solve;
+    if (transposed) op_csr = TransposedCsr(*plan);
+  } else {
+    const std::size_t flags = RoundUp(ascb_trsv_scratch_bytes(n), 256);
+    const std::int64_t nnz = m->nonzeros;
+    const std::size_t element = ascb::host::ElementBytes(m->element_kind);
+    std::size_t total = flags;
+    std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, sort = 0, outer_of = 0;
+    if (transposed && !alpha_zero) {
+      t_ptr = total;
+      total += RoundUp(static_cast<std::size_t>(n + 1) * 8, 256);
+      t_idx = total;
+      total += EntryBytes(nnz, 8);
+      t_perm = total;
+      total += EntryBytes(nnz, 8);
+      t_val = total;
+      total += EntryBytes(nnz, element);
+      sort = total;
+      total += RoundUp(ascb_sort_workspace_bytes(nnz, n), 256);
+      outer_of = total;
+      total += EntryBytes(nnz, 8);
+    }
+    s = SolveScratch(ctx, total, &control);
+    if (!s.ok()) return s;
+    if (transposed && !alpha_zero) {
+      auto* tp = reinterpret_cast<std::int64_t*>(control + t_ptr);
+      auto* ti = reinterpret_cast<std::int64_t*>(control + t_idx);
+      s = BuildTransposed(ctx, op_csr, element, tp, ti,
+                          reinterpret_cast<std::int64_t*>(control + t_perm), control + t_val,
+                          control + sort, reinterpret_cast<std::int64_t*>(control + outer_of));
+      if (!s.ok()) return s;
+      op_csr.ptr = tp;
+      op_csr.idx = ti;
+      op_csr.val = control + t_val;
+    }
+  }
+  ascb_trsv t{};
+  t.ptr = op_csr.ptr;
+  t.idx = op_csr.idx;
+  t.val = op_csr.val;
+  t.n = n;
+  t.lower = transposed ? triangle == ASC_SB_UPPER : triangle == ASC_SB_LOWER;
+  t.unit = diagonal == ASC_SB_UNIT;
+  t.conj = op == ASC_SB_OP_CONJUGATE_TRANSPOSE && !RealKind(m->element_kind);
+  t.row_major = rhs->layout == ASC_SB_ROW_MAJOR;
+  t.x = const_cast<void*>(rhs->data);
+  t.ld = rhs->leading_dimension;
+  t.k = rhs->columns;
+  t.control = control;
+  t.ready = reinterpret_cast<unsigned*>(control + 16);
+  t.status = ctx->status;
+  return Launched(ctx,
+                  ascb_sptrsv(ctx->stream, Dtype(m->element_kind),
+                              ctx->determinism == ASC_SB_DETERMINISTIC, alpha_zero, &t,
+                              alpha_real, alpha_imag, ctx->sm_count),
+                  "CUDA could not launch the triangular solve");
+}
+
+}  // namespace
+
+int asc_sb_standard_triangular_solve(asc_sb_context* ctx, int32_t op, double alpha_real,
+                                     double alpha_imag, const asc_sb_sparse* matrix,
+                                     int32_t triangle, int32_t diagonal,
+                                     const asc_sb_dense* right_hand_sides) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  return Finish(ctx, TriangularSolve(ctx, nullptr, op, alpha_real, alpha_imag, matrix, triangle,
+                                     diagonal, right_hand_sides));
+}
+
+int asc_sb_plan_triangular_solve(asc_sb_context* ctx, const asc_sb_plan* plan, int32_t op,
+                                 double alpha_real, double alpha_imag, int32_t triangle,
+                                 int32_t diagonal, const asc_sb_dense* right_hand_sides) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "null plan"));
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  return Finish(ctx, TriangularSolve(ctx, plan, op, alpha_real, alpha_imag, &plan->matrix,
+                                     triangle, diagonal, right_hand_sides));
 }
 
 // ---------------------------------------------------------------------------

@@ -302,6 +302,50 @@ def CudaSpmm(context: SparseCudaContext, op: SparseBlasTranspose, alpha: float,
         ctypes.byref(cd)))
 
 
+def CudaSparseTriangularSolveMultiple(context: SparseCudaContext, op: SparseBlasTranspose,
+                                      alpha: complex, matrix: CudaCsrArray, triangle: int,
+                                      diagonal: int, right_hand_sides: DenseMatrixView,
+                                      plan: "CsrPlan | None" = None) -> None:
+    """Solves op(A) X = alpha B in place (cuda.h:1727-1739 /
+    blas.h:1856-1910 semantics); with a plan, its triangular-solve state and
+    transposed structure are used."""
+    rd = right_hand_sides.describe()
+    a = complex(alpha)
+    if plan is not None:
+        context.check(context._lib.asc_sb_plan_triangular_solve(
+            context.handle, plan.handle, int(op), a.real, a.imag, int(triangle), int(diagonal),
+            ctypes.byref(rd)))
+        return
+    m = matrix.describe()
+    context.check(context._lib.asc_sb_standard_triangular_solve(
+        context.handle, int(op), a.real, a.imag, ctypes.byref(m), int(triangle), int(diagonal),
+        ctypes.byref(rd)))
+
+
+def CudaSparseTriangularSolve(context: SparseCudaContext, op: SparseBlasTranspose,
+                              alpha: complex, matrix: CudaCsrArray, triangle: int,
+                              diagonal: int, right_hand_side: CudaStridedVectorView,
+                              plan: "CsrPlan | None" = None) -> None:
+    """One right-hand side (cuda.h:1680-1705): the vector is passed as an
+    n x 1 row-major matrix whose leading dimension is its increment."""
+    v = right_hand_side
+    es = v.tensor.element_size()
+    view = DenseMatrixView(v.tensor, v.extent, 1, SparseBlasLayout.kRowMajor, v.stride,
+                           v.writable)
+    rd = view.describe()
+    rd.data = v.tensor.data_ptr() + v.offset * es if v.extent else None
+    a = complex(alpha)
+    if plan is not None:
+        context.check(context._lib.asc_sb_plan_triangular_solve(
+            context.handle, plan.handle, int(op), a.real, a.imag, int(triangle), int(diagonal),
+            ctypes.byref(rd)))
+        return
+    m = matrix.describe()
+    context.check(context._lib.asc_sb_standard_triangular_solve(
+        context.handle, int(op), a.real, a.imag, ctypes.byref(m), int(triangle), int(diagonal),
+        ctypes.byref(rd)))
+
+
 class CsrPlan:
     """Cached analysis of one device matrix (partitions, transposed structure),
     stored in a device buffer this object owns."""

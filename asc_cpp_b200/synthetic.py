@@ -17,6 +17,8 @@ Workloads:
 * :func:`stencil_27` - 27-point stencil on an ``m^3`` grid, values N(0,1).
 * :func:`block_sparse` - dense ``b x b`` blocks at a given block density.
 * :func:`banded_batch` - many banded matrices with sparse off-band fill.
+* :func:`triangular` - diagonally dominant triangular matrix, near-diagonal
+  plus long-range entries; :func:`triangle_of` - one triangle of a matrix.
 """
 
 from __future__ import annotations
@@ -316,3 +318,60 @@ def banded_batch_device(count: int = 4096, min_rows: int = 64, max_rows: int = 1
     torch.cuda.synchronize(device)
     return {"ptr": ptr, "idx": idx, "val": val, "x": x, "y": y, "rows": sizes, "nnz": nnz,
             "ptr_base": ptr_base, "nz_base": nz_base[:-1], "row_base": row_base[:-1]}
+
+
+def _values(rng: np.random.Generator, count: int, dtype) -> np.ndarray:
+    v = rng.uniform(-1.0, 1.0, size=count)
+    if np.iscomplexobj(np.zeros(1, dtype)):
+        v = v + 1j * rng.uniform(-1.0, 1.0, size=count)
+    return v.astype(dtype)
+
+
+def triangular(rng: np.random.Generator, n: int, lower: bool = True, near: int = 4,
+               far: int = 2, span: int = 64, dtype=np.float64,
+               diagonal: bool = True) -> Csr:
+    """Square triangular CSR: per row up to ``near`` entries within ``span``
+    of the diagonal and ``far`` anywhere in the strict triangle (duplicates
+    merged), values uniform in [-1, 1] (both parts for complex), and -- with
+    ``diagonal`` -- a diagonal of magnitude 1 + sum of the row's |entries| with
+    a random sign (a random phase for complex), so that solves stay well
+    conditioned."""
+    r = np.arange(n, dtype=np.int64)
+    off = rng.integers(1, span + 1, size=(n, near), dtype=np.int64)
+    cols_near = r[:, None] - off if lower else r[:, None] + off
+    u = rng.random((n, far))
+    if lower:
+        cols_far = np.floor(u * r[:, None]).astype(np.int64)
+        ok_far = r[:, None] > 0
+    else:
+        cols_far = r[:, None] + 1 + np.floor(u * (n - 1 - r)[:, None]).astype(np.int64)
+        ok_far = r[:, None] < n - 1
+    cols = np.concatenate([cols_near, cols_far], axis=1)
+    ok = np.concatenate([(cols_near >= 0) & (cols_near < n),
+                         np.broadcast_to(ok_far, cols_far.shape)], axis=1)
+    key = np.unique((r[:, None] * n + cols)[ok])
+    rows_of = key // n
+    off_val = _values(rng, key.size, dtype)
+    if diagonal:
+        mag = np.bincount(rows_of, weights=np.abs(off_val), minlength=n) + 1.0
+        if np.iscomplexobj(np.zeros(1, dtype)):
+            sign = np.exp(1j * rng.uniform(0.0, 2.0 * np.pi, size=n))
+        else:
+            sign = rng.choice(np.array([-1.0, 1.0]), size=n)
+        key = np.concatenate([key, r * n + r])
+        order = np.argsort(key, kind="stable")
+        key = key[order]
+        off_val = np.concatenate([off_val, (sign * mag).astype(dtype)])[order]
+        rows_of = key // n
+    ptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows_of, minlength=n), out=ptr[1:])
+    return Csr(n, n, ptr, key % n, off_val)
+
+
+def triangle_of(m: Csr, lower: bool = True) -> Csr:
+    """The lower (or upper) triangle of a square CSR matrix, diagonal included."""
+    rows_of = np.repeat(np.arange(m.rows, dtype=np.int64), np.diff(m.ptr))
+    keep = m.idx <= rows_of if lower else m.idx >= rows_of
+    ptr = np.zeros(m.rows + 1, dtype=np.int64)
+    np.cumsum(np.bincount(rows_of[keep], minlength=m.rows), out=ptr[1:])
+    return Csr(m.rows, m.cols, ptr, m.idx[keep], m.val[keep])

@@ -281,13 +281,41 @@ ASC_SB_API int asc_sb_standard_level1(asc_sb_context* context, int32_t operation
                                       const asc_sb_vector* dense,
                                       const asc_sb_vector* result);
 
+/* asc::SparseBlasTriangle / SparseBlasDiagonal, blas.h:117-134 */
+enum { ASC_SB_UPPER = 0, ASC_SB_LOWER = 1 };
+enum { ASC_SB_NON_UNIT = 0, ASC_SB_UNIT = 1 };
+
+/* Replaces internal_sparse_cuda::StandardTriangularSolveErased (cuda.h:250-253;
+ * operations.cc:1380-1451), behind CudaSparseTriangularSolve[Multiple]
+ * (cuda.h:1680-1739); CPU contract blas.h:1774-1910.  Solves
+ * op(A) X = alpha B in place for the square CSR matrix A and the n x k dense
+ * right-hand sides (a vector is n x 1 row major with the increment as leading
+ * dimension).  triangle names A's triangle; entries of the other strict
+ * triangle are ignored; with ASC_SB_NON_UNIT the stored diagonal divides (a
+ * missing one divides by zero).  alpha == 0 writes zeros without reading B.
+ * DETERMINISTIC: the reference's order and rounding, bit for bit (complex
+ * division by Smith's method as the facet's kernel does); BACKEND_DEFAULT:
+ * contracted sums within gamma_{m+2} of the row's terms.  One launch, sync
+ * free, waits bounded (asc_sb_context_device_status reads 1 if one gave up).  The ready
+ * flags live in a context-owned buffer that grows to the largest n (and, for
+ * op != none, also holds the transposed structure, rebuilt per call); use a
+ * plan to keep all memory caller-provided. */
+ASC_SB_API int asc_sb_standard_triangular_solve(asc_sb_context* context, int32_t op,
+                                                double alpha_real, double alpha_imag,
+                                                const asc_sb_sparse* matrix,
+                                                int32_t triangle, int32_t diagonal,
+                                                const asc_sb_dense* right_hand_sides);
+
 /* ---- analysis plans (no reference counterpart) ----------------------------
  * A plan caches, in caller-provided device memory, everything the kernels can
  * reuse across calls on one matrix: the row-tile and merge-path partitions and
  * (optionally) the transposed structure with its values.  The matrix's values
  * must not change while a plan built with ASC_SB_PLAN_TRANSPOSE is in use
  * (call asc_sb_plan_refresh_values after changing them). */
-enum { ASC_SB_PLAN_TRANSPOSE = 1 };
+/* ASC_SB_PLAN_TRIANGULAR adds the ready flags of triangular solves
+ * (asc_sb_plan_triangular_solve); solves through one plan must be ordered
+ * (one stream). */
+enum { ASC_SB_PLAN_TRANSPOSE = 1, ASC_SB_PLAN_TRIANGULAR = 2 };
 typedef struct asc_sb_plan asc_sb_plan;
 ASC_SB_API int asc_sb_plan_workspace_size(asc_sb_context* context,
                                           const asc_sb_sparse* matrix,
@@ -332,6 +360,16 @@ ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
                                          double alpha_real, double alpha_imag,
                                          const asc_sb_dense* input,
                                          const asc_sb_dense* output);
+
+/* Triangular solve through a plan created with ASC_SB_PLAN_TRIANGULAR: same
+ * contract as asc_sb_standard_triangular_solve on the plan's matrix; op !=
+ * none also needs ASC_SB_PLAN_TRANSPOSE (else ASC_SB_INVALID_STATE) and reuses
+ * the plan's transposed structure.  Allocates nothing. */
+ASC_SB_API int asc_sb_plan_triangular_solve(asc_sb_context* context,
+                                            const asc_sb_plan* plan, int32_t op,
+                                            double alpha_real, double alpha_imag,
+                                            int32_t triangle, int32_t diagonal,
+                                            const asc_sb_dense* right_hand_sides);
 
 /* ---- format conversion on the device --------------------------------------
  * Stable conversions of device data, bit-identical to the reference's host

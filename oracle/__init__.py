@@ -103,6 +103,14 @@ class Restatement:
             f.restype = None
             f.argtypes = [_INT, _INT, _P, _P, _I64, sc, sc, _P, _P]
         self.lib.oracle_output_counts.restype = None
+        for sfx, sc in (("f64", ctypes.c_double), ("f32", ctypes.c_float)):
+            f = getattr(self.lib, f"oracle_trsv_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _INT, _I64, _P, _P, _P, sc, _P, _INT, _I64, _I64]
+        for sfx, sc in (("z", ctypes.c_double), ("c", ctypes.c_float)):
+            f = getattr(self.lib, f"oracle_trsv_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _INT, _I64, _P, _P, _P, sc, sc, _P, _INT, _I64, _I64]
         self.lib.oracle_output_counts.argtypes = [_INT, _I64, _I64, _P, _P, _P]
         self.lib.oracle_csr_transpose_structure.restype = None
         self.lib.oracle_csr_transpose_structure.argtypes = [_I64, _I64, _P, _P,
@@ -204,6 +212,28 @@ class Restatement:
                 _ptr(res))
         return val, x, res[0]
 
+    def triangular_solve(self, op, triangle, diagonal, n, ptr, idx, val, alpha, b,
+                         layout=ROW_MAJOR, ld=None, k=1):
+        """Solves op(A) X = alpha B for square CSR A on a copy of the dense
+        storage ``b`` (n x k, ``layout``, ``ld``); returns the copy."""
+        b = np.array(b, copy=True)
+        ld = (k if layout == ROW_MAJOR else n) if ld is None else ld
+        cs = _complex_suffix(val.dtype)
+        if cs is not None:
+            rs = _real_scalar(val.dtype)
+            a = complex(alpha)
+            rc = getattr(self.lib, f"oracle_trsv_{cs}")(
+                op, triangle, diagonal, n, _ptr(ptr), _ptr(idx), _ptr(val), rs(a.real),
+                rs(a.imag), _ptr(b), layout, ld, k)
+        else:
+            sc = _scalar(val.dtype)
+            rc = getattr(self.lib, f"oracle_trsv_{_suffix(val.dtype)}")(
+                op, triangle, diagonal, n, _ptr(ptr), _ptr(idx), _ptr(val),
+                sc(float(np.real(alpha))), _ptr(b), layout, ld, k)
+        if rc != 0:
+            raise MemoryError("oracle triangular solve could not allocate")
+        return b
+
     def stable_bucket_sort(self, keys, kstride, n, limit):
         """(offsets[limit+1], perm[n]) of the stable sort of keys[e*kstride]."""
         offsets = np.zeros(limit + 1, dtype=np.int64)
@@ -288,6 +318,12 @@ class Reference:
             f = getattr(self.lib, f"ref_level1_{sfx}")
             f.restype = _INT
             f.argtypes = [_INT, _INT, _P, _P, _I64, _I64, sc, sc, _P, _P]
+        for sfx, sc in (("f64", ctypes.c_double), ("f32", ctypes.c_float),
+                        ("z", ctypes.c_double), ("c", ctypes.c_float)):
+            f = getattr(self.lib, f"ref_trsv_{sfx}")
+            f.restype = _INT
+            f.argtypes = [_INT, _INT, _INT, _I64, _P, _P, _P, _I64, sc, sc, _P, _INT, _I64,
+                          _I64, _SZ]
         f = self.lib.ref_convert_compressed_f64
         f.restype = _INT
         f.argtypes = [_INT, _I64, _I64, _P, _P, _P, _I64, _P, _P, _P]
@@ -407,3 +443,17 @@ class Reference:
         if rc != 0:
             raise RuntimeError(f"reference level-one failed with code {rc}")
         return val, x, res[0]
+
+    def triangular_solve(self, op, triangle, diagonal, n, ptr, idx, val, alpha, b,
+                         layout=ROW_MAJOR, ld=None, k=1):
+        """The reference's SparseTriangularSolveMultiple on a copy of ``b``;
+        returns (error code, solved copy)."""
+        b = np.array(b, copy=True)
+        ld = (k if layout == ROW_MAJOR else n) if ld is None else ld
+        sfx = _complex_suffix(val.dtype) or _suffix(val.dtype)
+        rs = _real_scalar(val.dtype) if _complex_suffix(val.dtype) else _scalar(val.dtype)
+        a = complex(alpha)
+        rc = getattr(self.lib, f"ref_trsv_{sfx}")(
+            op, triangle, diagonal, n, _ptr(ptr), _ptr(idx), _ptr(val), int(ptr[n]),
+            rs(a.real), rs(a.imag), _ptr(b), layout, ld, k, b.size)
+        return rc, b

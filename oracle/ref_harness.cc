@@ -13,6 +13,7 @@
 //                   include/asc/sparse/blas.h:1607-1667
 //   * standard SpMM asc::Spmm(ctx, op, alpha, CompressedSparseView, B, C)
 //                   include/asc/sparse/blas.h:1692-1750
+//   * triangular    asc::SparseTriangularSolveMultiple (blas.h:1856-1910)
 //   * conversions   asc::ConvertToCsr / ConvertToCsc (compressed.h:1676-1780)
 //                   -> CompressedSparseArray::FromCompressed (:1151-1221)
 //                   and FromCoordinate (:1082-1131)
@@ -386,6 +387,31 @@ int Level1(int op, int conj, const std::int64_t* idx, T* val, std::int64_t nnz,
   return Code(asc::SparseGatherZero(context, *dense, *sparse));
 }
 
+// Sparse triangular solve through the reference's SparseBlasTriangularView
+// (blas.h:1074-1160, which checks the triangle and, for a non-unit diagonal,
+// that every diagonal entry is stored and nonzero) and
+// SparseTriangularSolveMultiple (blas.h:1856-1910) on the n x k dense
+// right-hand sides b (layout 0 column major, 1 row major), solved in place.
+template <typename T>
+int TriangularSolve(int op, int triangle, int diagonal, std::int64_t n,
+                    const std::int64_t* ptr, const std::int64_t* idx, const T* val,
+                    std::int64_t nnz, T alpha, T* b, int layout, std::int64_t ld,
+                    std::int64_t k, std::size_t b_storage) {
+  const std::array<asc::extent_t, 2> shape{n, n};
+  auto m = asc::CsrView<const T>::Create(ptr, idx, val, shape, nnz, asc::MemorySpace::kHost);
+  if (!m.ok()) return Code(m.status());
+  auto tri = asc::SparseBlasTriangularView<T, asc::SparseCompressedFormat::kCsr>::Create(
+      *m, static_cast<asc::SparseBlasTriangle>(triangle),
+      static_cast<asc::SparseBlasDiagonal>(diagonal));
+  if (!tri.ok()) return Code(tri.status());
+  auto rhs = asc::SparseBlasMatrixView<T>::Create(
+      b, n, k, static_cast<asc::SparseBlasLayout>(layout), ld,
+      asc::MutableMemoryView(b, b_storage * sizeof(T), asc::MemorySpace::kHost));
+  if (!rhs.ok()) return Code(rhs.status());
+  return Code(asc::SparseTriangularSolveMultiple(asc::ExecutionContext::Serial(), Op(op), alpha,
+                                                 *tri, *rhs));
+}
+
 }  // namespace
 
 extern "C" {
@@ -551,5 +577,23 @@ ASC_REF_LEVEL1(f32, float, float)
 ASC_REF_LEVEL1(z, std::complex<double>, double)
 ASC_REF_LEVEL1(c, std::complex<float>, float)
 #undef ASC_REF_LEVEL1
+
+#define ASC_REF_TRSV(SUFFIX, T, R)                                              \
+  int ref_trsv_##SUFFIX(int op, int triangle, int diagonal, std::int64_t n,     \
+                        const std::int64_t* ptr, const std::int64_t* idx,       \
+                        const R* val, std::int64_t nnz, R alpha_re, R alpha_im, \
+                        R* b, int layout, std::int64_t ld, std::int64_t k,      \
+                        std::size_t b_storage) {                                \
+    return TriangularSolve<T>(op, triangle, diagonal, n, ptr, idx,              \
+                              reinterpret_cast<const T*>(val), nnz,             \
+                              MakeScalar<T>(alpha_re, alpha_im),                \
+                              reinterpret_cast<T*>(b), layout, ld, k,           \
+                              b_storage);                                       \
+  }
+ASC_REF_TRSV(f64, double, double)
+ASC_REF_TRSV(f32, float, float)
+ASC_REF_TRSV(z, std::complex<double>, double)
+ASC_REF_TRSV(c, std::complex<float>, float)
+#undef ASC_REF_TRSV
 
 }  // extern "C"

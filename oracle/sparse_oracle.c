@@ -396,3 +396,160 @@ void oracle_merge_path_split(int64_t rows, const int64_t* ptr, int64_t nnz,
   *row_out = lo;
   *nz_out = diagonal - lo;
 }
+
+/* ------------------------------------------------------------------------- */
+/* Sparse triangular solve op(A) X = alpha B, X overwriting B (n x k, dense
+ * layout/ld as in SpMM), for square CSR A.  Restates SparseTriangularSolve /
+ * SparseTriangularSolveMultiple (include/asc/sparse/blas.h:1774-1831,
+ * 1856-1910) and the CUDA facet's StandardTriangularSolveKernel
+ * (src/sparse/cuda/kernels.cu:349-391):
+ *   * alpha == 0: X = 0 (every element, both parts zero for complex);
+ *   * M = op(A); M is lower triangular when (op == none and triangle ==
+ *     lower) or (op != none and triangle == upper), and rows run 0..n-1 for
+ *     lower M, n-1..0 for upper M;
+ *   * value = alpha * B(row); then for each column c of the row's strict
+ *     triangle in increasing order value -= M(row, c) * X(c); with a non-unit
+ *     diagonal value /= M(row, row); X(row) = value.
+ * M(row, c) = A(c, row) for transposed ops, conjugated for the conjugate
+ * transpose.  The reference loops over every column and subtracts
+ * OpValue * X(c) with OpValue = 0 for entries that are not stored; this
+ * restatement visits stored entries only, which gives the same result
+ * whenever X holds finite values and no running value is a negative zero
+ * (a skipped 0 * x can only turn -0 into +0 or make Inf/NaN).  Stored
+ * entries outside the strict triangle other than the diagonal are ignored,
+ * as the CUDA facet ignores them.  A missing diagonal divides by zero, as
+ * the facet's CsrOpValue returns zero for it.
+ * Complex division follows the facet's DeviceArithmetic::Divide
+ * (kernels.cu:58-72), Smith's method (Smith, CACM 5(8), 1962): with
+ * d = dr + i di and |dr| >= |di|, r = di/dr, t = dr + di r,
+ * q = ((nr + ni r)/t, (ni - nr r)/t); otherwise r = dr/di, t = di + dr r,
+ * q = ((nr r + ni)/t, (ni r - nr)/t).                                       */
+enum { ORACLE_UPPER = 0, ORACLE_LOWER = 1 };
+enum { ORACLE_NON_UNIT = 0, ORACLE_UNIT = 1 };
+
+/* CSR of M = op(A): the stored arrays for op == none, else the stable
+ * transposed structure with values permuted.  Returns 0 on success. */
+static int oracle_op_csr(int op, int64_t n, const int64_t* ptr, const int64_t* idx,
+                         int64_t** m_ptr, int64_t** m_idx, int64_t** m_perm) {
+  const int64_t nnz = ptr[n];
+  *m_ptr = (int64_t*)malloc((size_t)(n + 1) * sizeof(int64_t));
+  *m_idx = (int64_t*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(int64_t));
+  *m_perm = (int64_t*)malloc((size_t)(nnz > 0 ? nnz : 1) * sizeof(int64_t));
+  if (*m_ptr == NULL || *m_idx == NULL || *m_perm == NULL) return -1;
+  if (op == ORACLE_OP_NONE) {
+    memcpy(*m_ptr, ptr, (size_t)(n + 1) * sizeof(int64_t));
+    for (int64_t p = 0; p < nnz; ++p) {
+      (*m_idx)[p] = idx[p];
+      (*m_perm)[p] = p;
+    }
+    return 0;
+  }
+  oracle_csr_transpose_structure(n, n, ptr, idx, *m_ptr, *m_idx, *m_perm);
+  return 0;
+}
+
+#define ORACLE_TRSV(SUFFIX, T)                                                 \
+  int oracle_trsv_##SUFFIX(int op, int triangle, int diagonal, int64_t n,      \
+                           const int64_t* ptr, const int64_t* idx,             \
+                           const T* val, T alpha, T* b, int layout, int64_t ld,\
+                           int64_t k) {                                        \
+    if (alpha == (T)0) {                                                       \
+      for (int64_t j = 0; j < k; ++j)                                          \
+        for (int64_t r = 0; r < n; ++r) b[dense_at(layout, ld, r, j)] = (T)0;  \
+      return 0;                                                                \
+    }                                                                          \
+    int64_t *mp, *mi, *mq;                                                     \
+    if (oracle_op_csr(op, n, ptr, idx, &mp, &mi, &mq) != 0) return -1;         \
+    const int lower = op == ORACLE_OP_NONE ? triangle == ORACLE_LOWER          \
+                                           : triangle == ORACLE_UPPER;         \
+    for (int64_t j = 0; j < k; ++j) {                                          \
+      for (int64_t s = 0; s < n; ++s) {                                        \
+        const int64_t row = lower ? s : n - 1 - s;                             \
+        T value = alpha * b[dense_at(layout, ld, row, j)];                     \
+        T diag = (T)0;                                                         \
+        for (int64_t p = mp[row]; p < mp[row + 1]; ++p) {                      \
+          const int64_t c = mi[p];                                             \
+          if (c == row) diag = val[mq[p]];                                     \
+          if ((lower && c >= row) || (!lower && c <= row)) continue;           \
+          value -= val[mq[p]] * b[dense_at(layout, ld, c, j)];                 \
+        }                                                                      \
+        if (diagonal == ORACLE_NON_UNIT) value /= diag;                        \
+        b[dense_at(layout, ld, row, j)] = value;                               \
+      }                                                                        \
+    }                                                                          \
+    free(mp);                                                                  \
+    free(mi);                                                                  \
+    free(mq);                                                                  \
+    return 0;                                                                  \
+  }
+ORACLE_TRSV(f64, double)
+ORACLE_TRSV(f32, float)
+
+#define ORACLE_TRSV_COMPLEX(SUFFIX, T)                                         \
+  static inline void cdiv_##SUFFIX(T nr, T ni, T dr, T di, T* qr, T* qi) {     \
+    const T adr = dr < (T)0 ? -dr : dr;                                        \
+    const T adi = di < (T)0 ? -di : di;                                        \
+    if (adr >= adi) {                                                          \
+      const T ratio = di / dr;                                                 \
+      const T den = dr + di * ratio;                                           \
+      *qr = (nr + ni * ratio) / den;                                           \
+      *qi = (ni - nr * ratio) / den;                                           \
+    } else {                                                                   \
+      const T ratio = dr / di;                                                 \
+      const T den = di + dr * ratio;                                           \
+      *qr = (nr * ratio + ni) / den;                                           \
+      *qi = (ni * ratio - nr) / den;                                           \
+    }                                                                          \
+  }                                                                            \
+  int oracle_trsv_##SUFFIX(int op, int triangle, int diagonal, int64_t n,      \
+                           const int64_t* ptr, const int64_t* idx,             \
+                           const T* val, T al_r, T al_i, T* b, int layout,     \
+                           int64_t ld, int64_t k) {                            \
+    if (al_r == (T)0 && al_i == (T)0) {                                        \
+      for (int64_t j = 0; j < k; ++j)                                          \
+        for (int64_t r = 0; r < n; ++r) {                                      \
+          const int64_t e = dense_at(layout, ld, r, j);                        \
+          b[2 * e] = (T)0;                                                     \
+          b[2 * e + 1] = (T)0;                                                 \
+        }                                                                      \
+      return 0;                                                                \
+    }                                                                          \
+    int64_t *mp, *mi, *mq;                                                     \
+    if (oracle_op_csr(op, n, ptr, idx, &mp, &mi, &mq) != 0) return -1;         \
+    const int lower = op == ORACLE_OP_NONE ? triangle == ORACLE_LOWER          \
+                                           : triangle == ORACLE_UPPER;         \
+    const int conj = op == ORACLE_OP_CONJ_TRANSPOSE;                           \
+    for (int64_t j = 0; j < k; ++j) {                                          \
+      for (int64_t s = 0; s < n; ++s) {                                        \
+        const int64_t row = lower ? s : n - 1 - s;                             \
+        const int64_t e = dense_at(layout, ld, row, j);                        \
+        T vr, vi;                                                              \
+        cmul_##SUFFIX(al_r, al_i, b[2 * e], b[2 * e + 1], &vr, &vi);           \
+        T dr = (T)0, di = (T)0;                                                \
+        for (int64_t p = mp[row]; p < mp[row + 1]; ++p) {                      \
+          const int64_t c = mi[p];                                             \
+          const T mr = val[2 * mq[p]];                                         \
+          const T mi_ = conj ? -val[2 * mq[p] + 1] : val[2 * mq[p] + 1];       \
+          if (c == row) {                                                      \
+            dr = mr;                                                           \
+            di = mi_;                                                          \
+          }                                                                    \
+          if ((lower && c >= row) || (!lower && c <= row)) continue;           \
+          const int64_t xe = dense_at(layout, ld, c, j);                       \
+          T pr, pi;                                                            \
+          cmul_##SUFFIX(mr, mi_, b[2 * xe], b[2 * xe + 1], &pr, &pi);          \
+          vr -= pr;                                                            \
+          vi -= pi;                                                            \
+        }                                                                      \
+        if (diagonal == ORACLE_NON_UNIT) cdiv_##SUFFIX(vr, vi, dr, di, &vr, &vi); \
+        b[2 * e] = vr;                                                         \
+        b[2 * e + 1] = vi;                                                     \
+      }                                                                        \
+    }                                                                          \
+    free(mp);                                                                  \
+    free(mi);                                                                  \
+    free(mq);                                                                  \
+    return 0;                                                                  \
+  }
+ORACLE_TRSV_COMPLEX(z, double)
+ORACLE_TRSV_COMPLEX(c, float)

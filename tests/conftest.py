@@ -37,6 +37,11 @@ def known_answers():
 
 
 @pytest.fixture(scope="session")
+def trsv_cases():
+    return dict(np.load(os.path.join(GOLDEN, "trsv_cases.npz")))
+
+
+@pytest.fixture(scope="session")
 def level1_cases():
     return dict(np.load(os.path.join(GOLDEN, "level1_cases.npz")))
 

@@ -36,6 +36,9 @@ into oracle/_ref/libasc_ref.so by oracle/build_oracle.py).  The fixtures pin:
   gather, gather-zero and scatter on the indexed vector of
   tests/sparse/standard_blas_test.cc:69-173 and on a seeded random one, for
   FP64, FP32, Z and C.
+* ``trsv_cases.npz`` - triangular solves: the reference tests' 2 x 2 and 1 x 1
+  cases and seeded random 48 x 48 triangular matrices for every triangle,
+  diagonal, op and right-hand-side shape, FP64/FP32/Z/C.
 
 Usage:  python tests/golden/make_golden.py
 """
@@ -53,7 +56,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 from asc_cpp_b200 import synthetic  # noqa: E402
-from oracle import (CSC, CSR, COL_MAJOR, OP_NONE, OP_TRANSPOSE,  # noqa: E402
+from oracle import (CSC, CSR, COL_MAJOR, OP_CONJ_TRANSPOSE, OP_NONE, OP_TRANSPOSE,  # noqa: E402
                     ROW_MAJOR, Reference, build_oracle)
 
 
@@ -305,6 +308,72 @@ def level1_cases(ref: Reference) -> dict[str, np.ndarray]:
     return out
 
 
+TRSV_TAGS = (("f64", np.float64), ("f32", np.float32), ("z", np.complex128),
+             ("c", np.complex64))
+TRSV_SHAPES = ((ROW_MAJOR, 1), (ROW_MAJOR, 3), (COL_MAJOR, 3))
+
+
+def trsv_cases(ref: Reference) -> dict[str, np.ndarray]:
+    """The reference's triangular solves (blas.h:1774-1910): the cases of
+    tests/sparse/standard_blas_test.cc:336-420 and
+    tests/sparse_cuda/standard_blas_cuda_test.cc:542-680 (the 2 x 2 lower
+    matrix with values 2+1i, 1-1i, 3+0.5i solved for (2, -1), its conjugate
+    transpose, two right-hand sides, alpha = 0 over NaN values, and the 1 x 1
+    complex matrix of magnitude 1e200 / 1e30 divided by itself), then seeded
+    random 48 x 48 triangular matrices for every triangle, diagonal, op and
+    right-hand-side shape (``rand_<tag>_<triangle><diagonal><op>_<shape>``)."""
+    out: dict[str, np.ndarray] = {}
+    rng = np.random.default_rng(67)
+    for tag, dt in TRSV_TAGS:
+        cplx = np.iscomplexobj(dt(0))
+        v = np.array([2 + 1j, 1 - 1j, 3 + 0.5j] if cplx else [2.0, 1.0, 3.0], dt)
+        ptr = np.array([0, 1, 3], np.int64)
+        idx = np.array([0, 0, 1], np.int64)
+        two, m1, one, three = dt(2), dt(-1), dt(1), dt(3)
+        cases = {
+            "vec": (OP_NONE, np.array([v[0] * two, v[1] * two + v[2] * m1], dt), 1),
+            "ct": (OP_CONJ_TRANSPOSE,
+                   np.array([np.conj(v[0]) * two - np.conj(v[1]), -np.conj(v[2])], dt), 1),
+            "multi": (OP_NONE, np.array([v[0] * two, v[0] * one, v[1] * two + v[2] * m1,
+                                         v[1] * one + v[2] * three], dt), 2),
+        }
+        for name, (op, b, k) in cases.items():
+            rc, x = ref.triangular_solve(op, 1, 0, 2, ptr, idx, v, 1.0, b, ROW_MAJOR, k, k)
+            _check(rc)
+            out[f"ka_{name}_{tag}_b"], out[f"ka_{name}_{tag}_x"] = b, x
+        out[f"ka_{tag}_val"] = v
+        nan = dt(complex(np.nan, np.nan)) if cplx else dt(np.nan)
+        zv = np.array([2, nan, 3], dt)
+        rc, x = ref.triangular_solve(OP_NONE, 1, 0, 2, ptr, idx, zv, 0.0,
+                                     np.array([4, 5], dt), ROW_MAJOR, 1, 1)
+        _check(rc)
+        out[f"ka_zero_{tag}_val"], out[f"ka_zero_{tag}_x"] = zv, x
+        if cplx:
+            big = 1e30 if dt == np.complex64 else 1e200
+            lv = np.array([complex(big, big)], dt)
+            rc, x = ref.triangular_solve(OP_NONE, 1, 0, 1, np.array([0, 1], np.int64),
+                                         np.array([0], np.int64), lv, 1.0, lv, ROW_MAJOR, 1, 1)
+            _check(rc)
+            out[f"ka_large_{tag}_val"], out[f"ka_large_{tag}_x"] = lv, x
+        for triangle in (0, 1):
+            for diagonal in (0, 1):
+                m = synthetic.triangular(rng, 48, lower=triangle == 1, near=3, far=2,
+                                         span=8, dtype=dt)
+                for op in (OP_NONE, OP_TRANSPOSE, OP_CONJ_TRANSPOSE):
+                    for s, (layout, k) in enumerate(TRSV_SHAPES):
+                        b = synthetic._values(rng, 48 * k, dt)
+                        alpha = (0.5 - 1.25j) if cplx else -1.5
+                        rc, x = ref.triangular_solve(op, triangle, diagonal, 48, m.ptr, m.idx,
+                                                     m.val, alpha, b, layout, None, k)
+                        _check(rc)
+                        key = f"rand_{tag}_{triangle}{diagonal}{op}_{s}"
+                        out[key + "_b"], out[key + "_x"] = b, x
+                out[f"rand_{tag}_{triangle}{diagonal}_ptr"] = m.ptr
+                out[f"rand_{tag}_{triangle}{diagonal}_idx"] = m.idx
+                out[f"rand_{tag}_{triangle}{diagonal}_val"] = m.val
+    return out
+
+
 def main() -> None:
     build_oracle.build_reference()
     ref = Reference()
@@ -314,8 +383,9 @@ def main() -> None:
     np.savez_compressed(os.path.join(HERE, "conversions.npz"), **conversions(ref))
     np.savez_compressed(os.path.join(HERE, "complex_cases.npz"), **complex_cases(ref))
     np.savez_compressed(os.path.join(HERE, "level1_cases.npz"), **level1_cases(ref))
+    np.savez_compressed(os.path.join(HERE, "trsv_cases.npz"), **trsv_cases(ref))
     for f in ("known_answers.npz", "random_cases.npz", "laplacian.npz", "conversions.npz",
-              "complex_cases.npz", "level1_cases.npz"):
+              "complex_cases.npz", "level1_cases.npz", "trsv_cases.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)))
 
 

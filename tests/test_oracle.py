@@ -6,6 +6,7 @@ where the reference harness is built, bit-exactly against it directly."""
 import numpy as np
 import pytest
 
+from asc_cpp_b200 import synthetic
 from oracle import CSC, CSR, COL_MAJOR, OP_NONE, OP_TRANSPOSE, ROW_MAJOR
 
 
@@ -312,3 +313,83 @@ def test_level1_known_answer_values(level1_cases):
     assert level1_cases["ka_op0_conj0_f64_res"][0] == -1.0
     assert level1_cases["ka_op1_conj0_f64_x"].tolist() == [5.0, 9.0, -2.0]
     assert level1_cases["ka_op3_conj0_f64_x"].tolist() == [0.0, 9.0, 0.0]
+
+
+TRSV_TAGS = {"f64": np.float64, "f32": np.float32, "z": np.complex128, "c": np.complex64}
+TRSV_SHAPES = ((1, 1), (1, 3), (0, 3))  # (layout: 1 row major / 0 column major, k)
+
+
+def trsv_fixture_cases(g, tag):
+    """(key, op, triangle, diagonal, layout, k, alpha, ptr, idx, val, b, x) of
+    the random triangular-solve fixtures of one element kind."""
+    dt = TRSV_TAGS[tag]
+    alpha = (0.5 - 1.25j) if np.iscomplexobj(dt(0)) else -1.5
+    for triangle in (0, 1):
+        for diagonal in (0, 1):
+            base = f"rand_{tag}_{triangle}{diagonal}"
+            ptr, idx, val = g[base + "_ptr"], g[base + "_idx"], g[base + "_val"]
+            for op in (0, 1, 2):
+                for s_, (layout, k) in enumerate(TRSV_SHAPES):
+                    key = f"{base}{op}_{s_}"
+                    yield (key, op, triangle, diagonal, layout, k, alpha, ptr, idx, val,
+                           g[key + "_b"], g[key + "_x"])
+
+
+@pytest.mark.parametrize("tag", list(TRSV_TAGS))
+def test_trsv_restatement_matches_reference_fixtures(restatement, trsv_cases, tag):
+    """The C restatement reproduces the reference's triangular solves bit for
+    bit, except complex FP32 division by a non-unit diagonal: the reference's
+    CPU build divides std::complex<float> with libgcc's routine, the
+    restatement (like the CUDA facet, kernels.cu:58-72) with Smith's method;
+    there the two agree to a few ulps."""
+    for (key, op, tri, diag, layout, k, alpha, ptr, idx, val, b,
+         x) in trsv_fixture_cases(trsv_cases, tag):
+        got = restatement.triangular_solve(op, tri, diag, 48, ptr, idx, val, alpha, b, layout,
+                                           None, k)
+        if tag == "c" and diag == 0:
+            np.testing.assert_allclose(got, x, rtol=2e-5, atol=2e-6, err_msg=key)
+        else:
+            assert _bits_equal(got, x), key
+
+
+@pytest.mark.parametrize("tag", list(TRSV_TAGS))
+def test_trsv_known_answers(restatement, trsv_cases, tag):
+    """standard_blas_test.cc:336-420 and standard_blas_cuda_test.cc:542-680:
+    (2, -1) for the vector and its conjugate transpose, [[2, 1], [-1, 3]] for
+    two right-hand sides, zeros for alpha = 0 over NaN values, 1 for the huge
+    1 x 1 complex division."""
+    g = trsv_cases
+    ptr = np.array([0, 1, 3], np.int64)
+    idx = np.array([0, 0, 1], np.int64)
+    v = g[f"ka_{tag}_val"]
+    for name, op, k, want in (("vec", 0, 1, [2, -1]), ("ct", 2, 1, [2, -1]),
+                              ("multi", 0, 2, [2, 1, -1, 3])):
+        x = g[f"ka_{name}_{tag}_x"]
+        assert np.allclose(x, want, rtol=1e-6)
+        got = restatement.triangular_solve(op, 1, 0, 2, ptr, idx, v, 1.0, g[f"ka_{name}_{tag}_b"],
+                                           1, k, k)
+        assert np.allclose(got, want, rtol=1e-6)
+    zero = restatement.triangular_solve(0, 1, 0, 2, ptr, idx, g[f"ka_zero_{tag}_val"], 0.0,
+                                        np.array([4, 5], v.dtype), 1, 1, 1)
+    assert _bits_equal(zero, g[f"ka_zero_{tag}_x"]) and not zero.any()
+    if f"ka_large_{tag}_val" in g:
+        lv = g[f"ka_large_{tag}_val"]
+        got = restatement.triangular_solve(0, 1, 0, 1, np.array([0, 1], np.int64),
+                                           np.array([0], np.int64), lv, 1.0, lv, 1, 1, 1)
+        assert got[0] == 1 and g[f"ka_large_{tag}_x"][0] == 1
+
+
+def test_trsv_restatement_matches_reference_larger(restatement, reference):
+    """A 300 x 300 case per kind against the compiled reference (its solve
+    scans every stored entry per lookup, so larger ones take long)."""
+    rng = np.random.default_rng(3)
+    for dt in TRSV_TAGS.values():
+        for triangle, op in ((1, 0), (0, 2)):
+            m = synthetic.triangular(rng, 300, lower=triangle == 1, dtype=dt)
+            b = synthetic._values(rng, 600, dt)
+            rc, want = reference.triangular_solve(op, triangle, 1, 300, m.ptr, m.idx, m.val,
+                                                  1.0, b, 1, None, 2)
+            assert rc == 0
+            got = restatement.triangular_solve(op, triangle, 1, 300, m.ptr, m.idx, m.val, 1.0,
+                                               b, 1, None, 2)
+            assert _bits_equal(got, want)
