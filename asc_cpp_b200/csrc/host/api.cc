@@ -78,8 +78,15 @@ struct asc_sb_plan {
   // FP32 CSR made of dense, aligned 16 x 16 blocks: SpMM runs on the tensor
   // cores in BACKEND_DEFAULT mode
   bool block16 = false;
-  // ASC_SB_PLAN_TRIANGULAR: control block and ready flags of the solves
+  // ASC_SB_PLAN_TRIANGULAR: control block and published values of the
+  // solves, and room for one level analysis (asc_sb_plan_triangular_analysis)
   unsigned char* solve = nullptr;
+  unsigned char* analysis = nullptr;
+  bool analysed = false;
+  bool analysis_transposed = false;  // analysis of op != none
+  bool analysis_lower = false;       // of a lower triangular op(A)
+  const std::int64_t* order = nullptr;
+  const std::int64_t* position = nullptr;
 };
 
 namespace {
@@ -316,7 +323,7 @@ std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
 struct PlanLayout {
   std::size_t flag = 0;  // one device int for structure checks
   std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, t_part = 0;
-  std::size_t sort = 0, outer_of = 0, solve = 0, total = 0;
+  std::size_t sort = 0, outer_of = 0, solve = 0, analysis = 0, total = 0;
 };
 
 PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
@@ -346,7 +353,11 @@ PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
   }
   if (flags & ASC_SB_PLAN_TRIANGULAR) {
     l.solve = at;
-    at += RoundUp(ascb_trsv_scratch_bytes(outer), 256);
+    at += RoundUp(ascb_trsv_scratch_bytes(
+                      outer, static_cast<int>(ascb::host::ElementBytes(m.element_kind))),
+                  256);
+    l.analysis = at;
+    at += RoundUp(ascb_trsv_analysis_bytes(outer), 256);
   }
   l.total = at;
   return l;
@@ -942,7 +953,10 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
                         reinterpret_cast<std::int64_t*>(ws + l.outer_of));
     if (s.ok()) s = BuildPartitions(ctx, TransposedCsr(*plan), ws + l.t_part, &plan->t_part);
   }
-  if (flags & ASC_SB_PLAN_TRIANGULAR) plan->solve = ws + PlanLayoutFor(*m, flags).solve;
+  if (flags & ASC_SB_PLAN_TRIANGULAR) {
+    plan->solve = ws + PlanLayoutFor(*m, flags).solve;
+    plan->analysis = ws + PlanLayoutFor(*m, flags).analysis;
+  }
   if (s.ok() && m->format == ASC_SB_CSR && m->element_kind == ASC_SB_FLOAT && m->rows > 0 &&
       m->rows % 16 == 0 && m->nonzeros > 0 &&
       (reinterpret_cast<std::uintptr_t>(m->values) & 15u) == 0) {
@@ -1412,9 +1426,10 @@ Status TriangularSolve(asc_sb_context* ctx, const asc_sb_plan* plan, int op, dou
     control = plan->solve;
     if (transposed) op_csr = TransposedCsr(*plan);
   } else {
-    const std::size_t flags = RoundUp(ascb_trsv_scratch_bytes(n), 256);
-    const std::int64_t nnz = m->nonzeros;
     const std::size_t element = ascb::host::ElementBytes(m->element_kind);
+    const std::size_t flags =
+        RoundUp(ascb_trsv_scratch_bytes(n, static_cast<int>(element)), 256);
+    const std::int64_t nnz = m->nonzeros;
     std::size_t total = flags;
     std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, sort = 0, outer_of = 0;
     if (transposed && !alpha_zero) {
@@ -1458,7 +1473,12 @@ Status TriangularSolve(asc_sb_context* ctx, const asc_sb_plan* plan, int op, dou
   t.ld = rhs->leading_dimension;
   t.k = rhs->columns;
   t.control = control;
-  t.ready = reinterpret_cast<unsigned*>(control + 16);
+  t.pub = control + 16;
+  if (plan != nullptr && plan->analysed && plan->analysis_transposed == transposed &&
+      plan->analysis_lower == (t.lower != 0)) {
+    t.order = plan->order;
+    t.position = plan->position;
+  }
   t.status = ctx->status;
   return Launched(ctx,
                   ascb_sptrsv(ctx->stream, Dtype(m->element_kind),
@@ -1480,6 +1500,55 @@ int asc_sb_standard_triangular_solve(asc_sb_context* ctx, int32_t op, double alp
   if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
   return Finish(ctx, TriangularSolve(ctx, nullptr, op, alpha_real, alpha_imag, matrix, triangle,
                                      diagonal, right_hand_sides));
+}
+
+int asc_sb_plan_triangular_analysis(asc_sb_context* ctx, asc_sb_plan* plan, int32_t op,
+                                    int32_t triangle) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "null plan"));
+  if (op != ASC_SB_OP_NONE && op != ASC_SB_OP_TRANSPOSE && op != ASC_SB_OP_CONJUGATE_TRANSPOSE) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse BLAS transpose mode is invalid"));
+  }
+  if (triangle != ASC_SB_UPPER && triangle != ASC_SB_LOWER) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "A sparse BLAS triangle value is invalid"));
+  }
+  const asc_sb_sparse& m = plan->matrix;
+  if (m.format != ASC_SB_CSR || m.rows != m.columns) {
+    return Finish(ctx, Fail(ASC_SB_SHAPE, "CUDA triangular solve requires square CSR storage"));
+  }
+  const bool transposed = op != ASC_SB_OP_NONE;
+  if (plan->analysis == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_STATE, "the plan holds no triangular-solve state"));
+  }
+  if (transposed && plan->t_ptr == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_STATE,
+                            "a transposed solve needs a plan with the transposed structure"));
+  }
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  const ascb_csr op_csr = transposed ? TransposedCsr(*plan) : AsCsr(m, false);
+  ascb_trsv t{};
+  t.ptr = op_csr.ptr;
+  t.idx = op_csr.idx;
+  t.n = m.rows;
+  t.lower = transposed ? triangle == ASC_SB_UPPER : triangle == ASC_SB_LOWER;
+  t.control = plan->solve;
+  t.status = ctx->status;
+  std::int64_t* order = nullptr;
+  std::int64_t* position = nullptr;
+  plan->analysed = false;
+  s = Launched(ctx, ascb_trsv_analysis(ctx->stream, &t, plan->analysis, &order, &position,
+                                       ctx->sm_count),
+               "CUDA could not launch the triangular-solve analysis");
+  if (!s.ok()) return Finish(ctx, s);
+  plan->order = order;
+  plan->position = position;
+  plan->analysis_transposed = transposed;
+  plan->analysis_lower = t.lower != 0;
+  plan->analysed = true;
+  return Finish(ctx, Status::Ok());
 }
 
 int asc_sb_plan_triangular_solve(asc_sb_context* ctx, const asc_sb_plan* plan, int32_t op,

@@ -176,11 +176,12 @@ int ascb_level1(void* stream, int dtype, int op, int conj, int exact, const int6
 // ---- sparse triangular solve op(A) X = alpha B, X over B ----
 // ptr/idx/val: CSR of M = op(A) (n x n, sorted columns; values already those
 // of op(A) up to conjugation, applied when conj = 1).  lower: M is lower
-// triangular (rows solved 0..n-1), else upper (n-1..0).  x: the n x k dense
-// right-hand sides, element (r, j) at r*ld + j (row_major) or j*ld + r.
-// control: ascb_trsv_scratch_bytes(n) device bytes, 16-byte aligned, cleared
-// by the call on the stream; status (nullable) receives 1 if a bounded wait
-// gave up.
+// triangular (rows solved 0..n-1), else upper (n-1..0); order/position
+// (nullable, from ascb_trsv_analysis) replace that order by a level order.
+// x: the n x k dense right-hand sides, element (r, j) at r*ld + j (row_major)
+// or j*ld + r.  control: ascb_trsv_scratch_bytes(n, element bytes) device
+// bytes, 16-byte aligned, prepared by the call on the stream; pub = control +
+// 16 bytes.  status (nullable) receives 1 if a bounded wait gave up.
 typedef struct ascb_trsv {
   const int64_t* ptr;
   const int64_t* idx;
@@ -191,14 +192,23 @@ typedef struct ascb_trsv {
   int64_t ld;
   int64_t k;
   void* control;
-  unsigned* ready;  // (unsigned*)control + 4
+  void* pub;
+  const int64_t* order;
+  const int64_t* position;
   int* status;
 } ascb_trsv;
-size_t ascb_trsv_scratch_bytes(int64_t n);
+size_t ascb_trsv_scratch_bytes(int64_t n, int elem_bytes);
 // exact = 1: the reference's order and rounding (DETERMINISTIC).
 // alpha_is_zero = 1: X = 0 without reading it.
 int ascb_sptrsv(void* stream, int dtype, int exact, int alpha_is_zero, const ascb_trsv* t,
                 double alpha_re, double alpha_im, int sm_count);
+// Level order of M (t: ptr, idx, n, lower, control, status): rows sorted by
+// dependency level, stable by row.  workspace: ascb_trsv_analysis_bytes(n),
+// 256-byte aligned; *order / *position point into it (solve position -> row
+// and row -> solve position).
+size_t ascb_trsv_analysis_bytes(int64_t n);
+int ascb_trsv_analysis(void* stream, const ascb_trsv* t, void* workspace, int64_t** order,
+                       int64_t** position, int sm_count);
 
 // ---- SpMM: C += alpha * op(A) * B (k right-hand sides) ----
 // transpose = 0: stored-order row kernels (exact = 1: the reference's order

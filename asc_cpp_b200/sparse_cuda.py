@@ -376,6 +376,12 @@ class CsrPlan:
         self.context.check(self.context._lib.asc_sb_plan_properties(self._h, ctypes.byref(v)))
         return v.value
 
+    def triangular_analysis(self, op: SparseBlasTranspose, triangle: int) -> None:
+        """Level order for solves with this op class and triangle (plans
+        created with ASC_SB_PLAN_TRIANGULAR)."""
+        self.context.check(self.context._lib.asc_sb_plan_triangular_analysis(
+            self.context.handle, self._h, int(op), int(triangle)))
+
     def refresh_values(self) -> None:
         """Re-gathers the transposed values after the matrix's values changed."""
         self.context.check(self.context._lib.asc_sb_plan_refresh_values(

@@ -370,7 +370,10 @@ def run_gpu(args, rank, world):
 
 EXTRA = ("spmv_powerlaw_4M_f32", "spmv_t_powerlaw_4M_f64", "spmv_t_powerlaw_4M_f32",
          "spmm_stencil_k8", "spmm_stencil_k32", "spmm_stencil_k128",
-         "spmm_block_k8", "spmm_block_k32", "spmm_block_k128", "batched_banded_4096")
+         "spmm_block_k8", "spmm_block_k32", "spmm_block_k128", "batched_banded_4096",
+         "sptrsv_laplacian_1M_f64", "sptrsv_stencil27_2M_f64", "sptrsv_powerlaw_4M_f64",
+         "sptrsv_random_2M_f64", "sptrsv_random_2M_f32",
+         "level1_16M_f64")
 
 
 def _timer(stream, steps, warmup):
@@ -465,6 +468,116 @@ def run_extra(args):
         plan.close()
         dtype_s = "f32"
         extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "k": k, "layout": "row-major, ld=k"})
+    elif w.startswith("sptrsv"):
+        from asc_cpp_b200._abi import PLAN_TRIANGULAR, SparseBlasDiagonal, SparseBlasTriangle
+        dt = np.float32 if w.endswith("f32") else np.float64
+        es = np.dtype(dt).itemsize
+        unit_diagonal = False
+        if "laplacian" in w:
+            a_h = synthetic.triangle_of(synthetic.laplacian_2d(1000, dtype=dt))
+            extra_cfg["wavefronts"] = 2 * 1000 - 1
+        elif "stencil27" in w or "powerlaw" in w:
+            full = (synthetic.stencil_27(128, dtype=dt) if "stencil27" in w else
+                    synthetic.power_law(4_194_304, 16.0, 1.5, 65_536, seed=1, dtype=dt))
+            a_h = synthetic.triangle_of(full)
+            rows_of = np.repeat(np.arange(a_h.rows), np.diff(a_h.ptr))
+            on = a_h.idx == rows_of
+            mag = np.bincount(rows_of[~on], weights=np.abs(a_h.val[~on]), minlength=a_h.rows)
+            if "stencil27" in w:
+                # diagonally dominant: |diagonal| = 1 + sum of the other |entries|
+                a_h.val[on] = (1.0 + mag[rows_of[on]]).astype(dt)
+                extra_cfg["wavefronts"] = 3 * 127 + 1
+            else:
+                # the power-law matrix stores almost no diagonal: unit diagonal,
+                # entries scaled to row sums below 1/2
+                unit_diagonal = True
+                a_h.val[:] = (a_h.val / (2.0 * (mag[rows_of] + 1.0))).astype(dt)
+        else:
+            a_h = synthetic.triangular(np.random.default_rng(11), 2_000_000, lower=True, near=4,
+                                       far=2, span=64, dtype=dt)
+        n = a_h.rows
+        diag = SparseBlasDiagonal.kUnit if unit_diagonal else SparseBlasDiagonal.kNonUnit
+        extra_cfg["diagonal"] = "unit" if unit_diagonal else "non-unit"
+        with torch.cuda.stream(stream):
+            A = sc.CudaCsrArray(n, n, torch.from_numpy(a_h.ptr).to(dev),
+                                torch.from_numpy(a_h.idx).to(dev), torch.from_numpy(a_h.val).to(dev))
+            b0 = (torch.rand(n, device=dev, dtype=torch.float64) * 2 - 1).to(A.values.dtype)
+            xb = b0.clone()
+        stream.synchronize()
+        plan = sc.CsrPlan(ctx, A, PLAN_TRIANGULAR)
+        rhs = sc.DenseMatrixView(xb, n, 1)
+        # the solve overwrites its right-hand side: each step restores it
+        # (a device copy of n elements, inside the timed region)
+        byts = a_h.nnz * (es + 8) + (n + 1) * 8 + 2 * n * es
+
+        def solve(use_plan):
+            xb.copy_(b0)
+            sc.CudaSparseTriangularSolveMultiple(ctx, SparseBlasTranspose.kNone, 1.0, A,
+                                                 SparseBlasTriangle.kLower, diag, rhs,
+                                                 plan=plan if use_plan else None)
+        copy_ms = timed(lambda: xb.copy_(b0))
+        for name, det, use_plan in (("deterministic", Determinism.kDeterministic, False),
+                                    ("default", Determinism.kBackendDefault, False)):
+            ctx.set_determinism(det)
+            ms = timed(lambda: solve(use_plan)) - copy_ms
+            detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1)}
+        t0 = time.perf_counter()
+        plan.triangular_analysis(SparseBlasTranspose.kNone, SparseBlasTriangle.kLower)
+        stream.synchronize()
+        extra_cfg["analysis_ms"] = round((time.perf_counter() - t0) * 1e3, 3)
+        for name, det in (("deterministic_levels", Determinism.kDeterministic),
+                          ("default_levels", Determinism.kBackendDefault)):
+            ctx.set_determinism(det)
+            ms = timed(lambda: solve(True)) - copy_ms
+            detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1)}
+        plan.close()
+        try:  # the library baseline: cuSPARSE SpSV through torch (not on the product path)
+            At = torch.sparse_csr_tensor(A.offsets, A.indices, A.values, (n, n))
+            with torch.cuda.stream(stream):
+                ms = timed(lambda: torch.triangular_solve(b0.view(n, 1), At, upper=False,
+                                                          unitriangular=unit_diagonal))
+            detail["cusparse_spsv_via_torch"] = {"ms": round(ms, 4),
+                                                 "gbs": round(byts / ms / 1e6, 1)}
+        except Exception as e:  # noqa: BLE001
+            detail["cusparse_spsv_via_torch"] = {"unavailable": str(e).splitlines()[0][:120]}
+        from oracle import Restatement  # the CPU leg only (the oracle as the baseline)
+        r = Restatement()
+        bh = b0.cpu().numpy()
+        t0 = time.perf_counter()
+        r.triangular_solve(0, 1, int(diag), n, a_h.ptr, a_h.idx, a_h.val, 1.0, bh)
+        detail["cpu_oracle_1_thread"] = {"ms": round((time.perf_counter() - t0) * 1e3, 2)}
+        dtype_s = "f32" if dt == np.float32 else "f64"
+        extra_cfg.update({"rows": n, "nnz": a_h.nnz, "op": "none", "triangle": "lower",
+                          "rhs_restore_ms_subtracted": round(copy_ms, 4)})
+    elif w.startswith("level1"):
+        from asc_cpp_b200._abi import Level1Op
+        n, nnz = 64 * 1024 * 1024, 16 * 1024 * 1024
+        g = torch.Generator(device=dev)
+        g.manual_seed(3)
+        with torch.cuda.stream(stream):
+            idx = torch.sort(torch.randperm(n, device=dev, generator=g)[:nnz]).values
+            val = torch.rand(nnz, device=dev, dtype=torch.float64, generator=g)
+            x = torch.rand(n, device=dev, dtype=torch.float64, generator=g)
+            res = torch.zeros(1, device=dev, dtype=torch.float64)
+        stream.synchronize()
+        # bytes: index + value per entry, plus the 32-byte sectors of x touched
+        sectors = int(torch.unique(idx // 4).numel()) * 32
+        op_bytes = {"dot": nnz * 16 + sectors, "axpy": nnz * 16 + 2 * sectors,
+                    "gather": nnz * 24 + sectors, "scatter": nnz * 16 + sectors}
+        dv = sc.CudaStridedVectorView(x, n)
+        for name, op, det in (("dot_deterministic", Level1Op.kDot, Determinism.kDeterministic),
+                              ("dot_default", Level1Op.kDot, Determinism.kBackendDefault),
+                              ("axpy", Level1Op.kAxpy, Determinism.kDeterministic),
+                              ("gather", Level1Op.kGather, Determinism.kDeterministic),
+                              ("scatter", Level1Op.kScatter, Determinism.kDeterministic)):
+            ctx.set_determinism(det)
+            ms = timed(lambda: sc.CudaLevel1(ctx, op, idx, val, dv, res, 1e-9))
+            b = op_bytes[name.split("_")[0]]
+            detail[name] = {"ms": round(ms, 4), "gbs": round(b / ms / 1e6, 1)}
+        byts = op_bytes["axpy"]
+        detail = {"axpy": detail.pop("axpy"), **detail}
+        dtype_s = "f64"
+        extra_cfg.update({"dense": n, "nnz": nnz, "x_sectors_bytes": sectors})
     else:  # batched
         g = synthetic.banded_batch_device(4096)
         mats, xs, ys = [], [], []
@@ -492,7 +605,11 @@ def run_extra(args):
         batch.close()
         dtype_s = "f64"
         extra_cfg.update({"matrices": 4096, "rows": int(g["rows"].sum()), "nnz": int(g["nnz"].sum())})
-    best = min(detail, key=lambda k: detail[k]["ms"])
+    if w.startswith("level1"):
+        best = "axpy"
+    else:
+        best = min((k for k in detail if "ms" in detail[k] and not k.startswith(("cusparse", "cpu"))),
+                   key=lambda k: detail[k]["ms"])
     ms = detail[best]["ms"]
     gbs = byts / ms / 1e6
     out = {"metric": METRIC, "value": round(gbs, 3), "unit": "GB/s", "n_gpus": 1,

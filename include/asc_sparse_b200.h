@@ -364,7 +364,14 @@ ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
 /* Triangular solve through a plan created with ASC_SB_PLAN_TRIANGULAR: same
  * contract as asc_sb_standard_triangular_solve on the plan's matrix; op !=
  * none also needs ASC_SB_PLAN_TRANSPOSE (else ASC_SB_INVALID_STATE) and reuses
- * the plan's transposed structure.  Allocates nothing. */
+ * the plan's transposed structure.  Allocates nothing.  After
+ * asc_sb_plan_triangular_analysis for the same op class (none / transposed)
+ * and triangle, rows are scheduled in dependency-level order, which keeps
+ * wide wavefronts (e.g. grid stencils) in flight at once; the arithmetic and
+ * its results are unchanged. */
+ASC_SB_API int asc_sb_plan_triangular_analysis(asc_sb_context* context,
+                                               asc_sb_plan* plan, int32_t op,
+                                               int32_t triangle);
 ASC_SB_API int asc_sb_plan_triangular_solve(asc_sb_context* context,
                                             const asc_sb_plan* plan, int32_t op,
                                             double alpha_real, double alpha_imag,

@@ -208,6 +208,44 @@ def test_plan_solves_match_unplanned(cuda_lib, restatement):
     ctx.close()
 
 
+@pytest.mark.parametrize("det", [Determinism.kDeterministic, Determinism.kBackendDefault])
+def test_level_order_analysis(cuda_lib, restatement, det):
+    """After asc_sb_plan_triangular_analysis the plan's solves run in level
+    order and give the same bits as the row-order solve, for matching and
+    for mismatching (ignored) analyses, one and three right-hand sides."""
+    rng = np.random.default_rng(53)
+    ctx = context(det)
+    lap = synthetic.triangle_of(synthetic.laplacian_2d(300))
+    rand = synthetic.triangular(rng, 100_000, lower=True, near=3, far=3, span=5000,
+                                dtype=np.complex128)
+    for m in (lap, rand):
+        n = m.rows
+        a = csr(n, n, m.ptr, m.idx, m.val)
+        plan = CsrPlan(ctx, a, PLAN_TRANSPOSE | PLAN_TRIANGULAR)
+        for op, tri in ((SparseBlasTranspose.kNone, SparseBlasTriangle.kLower),
+                        (SparseBlasTranspose.kConjugateTranspose, SparseBlasTriangle.kLower)):
+            for k, layout in ((1, 1), (3, 0)):
+                b = synthetic._values(rng, n * k, m.val.dtype)
+                want = _solve(ctx, op, 1.5, a, tri, SparseBlasDiagonal.kNonUnit, b, n, k, layout)
+                plan.triangular_analysis(op, tri)
+                got = _solve(ctx, op, 1.5, a, tri, SparseBlasDiagonal.kNonUnit, b, n, k, layout,
+                             plan=plan)
+                assert bits_equal(got, want), (op, k)
+                if det == Determinism.kDeterministic:
+                    ref = restatement.triangular_solve(int(op), int(tri), 0, n, m.ptr, m.idx,
+                                                       m.val, 1.5, b, layout, None, k)
+                    assert bits_equal(got, ref)
+        # an analysis of the other op class is not used, and nothing changes
+        plan.triangular_analysis(SparseBlasTranspose.kTranspose, SparseBlasTriangle.kLower)
+        b = synthetic._values(rng, n, m.val.dtype)
+        assert bits_equal(_solve(ctx, SparseBlasTranspose.kNone, 1.0, a, SparseBlasTriangle.kLower,
+                                 SparseBlasDiagonal.kNonUnit, b, n, 1, 1, plan=plan),
+                          _solve(ctx, SparseBlasTranspose.kNone, 1.0, a, SparseBlasTriangle.kLower,
+                                 SparseBlasDiagonal.kNonUnit, b, n, 1, 1))
+        plan.close()
+    ctx.close()
+
+
 def test_strided_vector_and_padding(cuda_lib, restatement):
     """A vector with increment 3 (the reference's vector binding): only its
     elements change; the padding between them is never written."""
