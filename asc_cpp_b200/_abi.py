@@ -190,6 +190,9 @@ SIGNATURES: dict[str, tuple] = {
                                                         _DP]),
     "asc_sb_plan_triangular_solve": (ctypes.c_int, [_P, _P, _I32, _D, _D, _I32, _I32, _DP]),
     "asc_sb_plan_triangular_analysis": (ctypes.c_int, [_P, _P, _I32, _I32]),
+    "asc_sb_clone_csr": (ctypes.c_int, [_P, _SP, _SP]),
+    "asc_sb_clone_indexed": (ctypes.c_int, [_P, ctypes.POINTER(IndexedDesc),
+                                            ctypes.POINTER(IndexedDesc)]),
     "asc_sb_standard_level1": (ctypes.c_int, [_P, _I32, _I32, _D, _D,
                                               ctypes.POINTER(IndexedDesc), _VP, _VP]),
     "asc_sb_selector_param_count": (ctypes.c_int64, [_I32]),

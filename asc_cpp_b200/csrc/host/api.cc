@@ -48,6 +48,7 @@ struct asc_sb_context {
   // solve seen
   void* solve_scratch = nullptr;
   std::size_t solve_bytes = 0;
+  void* stager = nullptr;  // clone staging, clone.cc
 };
 
 constexpr std::size_t kContextScratchOffset = 256;
@@ -545,6 +546,7 @@ int asc_sb_context_destroy(asc_sb_context* ctx) {
   if (ctx->status != nullptr) (void)cudaFree(ctx->status);
   if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
   if (ctx->solve_scratch != nullptr) (void)cudaFree(ctx->solve_scratch);
+  ascb::host::DestroyStager(ctx->stager);
   delete ctx;
   return ASC_SB_OK;
 }
@@ -1779,6 +1781,7 @@ bool ViewContext(asc_sb_context* ctx, ContextView* view) {
   view->mutex = &ctx->mutex;
   view->last_error = &ctx->last_error;
   view->launches = &ctx->launches;
+  view->stager = &ctx->stager;
   return true;
 }
 

@@ -20,9 +20,12 @@ struct ContextView {
   std::mutex* mutex = nullptr;
   std::string* last_error = nullptr;
   std::atomic<std::int64_t>* launches = nullptr;
+  void** stager = nullptr;  // clone staging (clone.cc), created on first use
 };
 
 // False for a null context.
 bool ViewContext(asc_sb_context* context, ContextView* view);
+// Releases a context's clone staging (pinned buffers, copy threads).
+void DestroyStager(void* stager);
 
 }  // namespace ascb::host

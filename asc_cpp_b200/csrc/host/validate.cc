@@ -79,6 +79,20 @@ Status ValidateSparse(const asc_sb_sparse& m, int device, SparseBytes* out) {
   if (m.memory_space != ASC_SB_DEVICE) {
     return Fail(ASC_SB_MEMORY_ACCESS, "Sparse CUDA operations require device storage");
   }
+  SparseBytes b;
+  Status s = ValidateSparseMetadata(m, &b);
+  if (!s.ok()) return s;
+  for (const Span& span : {Span{m.structure_first, b.first}, Span{m.structure_second, b.second},
+                           Span{m.values, b.values}}) {
+    s = ValidateDevicePointer(span.begin, span.bytes, device,
+                              "CUDA could not inspect sparse operand storage");
+    if (!s.ok()) return s;
+  }
+  if (out) *out = b;
+  return Status::Ok();
+}
+
+Status ValidateSparseMetadata(const asc_sb_sparse& m, SparseBytes* out) {
   if (m.format != ASC_SB_CSR && m.format != ASC_SB_CSC) {
     return Fail(ASC_SB_INVALID_ARGUMENT, "Sparse CUDA SpMV/SpMM requires CSR or CSC format");
   }
@@ -128,11 +142,6 @@ Status ValidateSparse(const asc_sb_sparse& m, int device, SparseBytes* out) {
   if (Overlap(first, second) || Overlap(first, values) || Overlap(second, values)) {
     return Fail(ASC_SB_INVALID_ARGUMENT,
                 "Sparse CUDA descriptor storage spans cannot overlap");
-  }
-  for (const Span& span : {first, second, values}) {
-    s = ValidateDevicePointer(span.begin, span.bytes, device,
-                              "CUDA could not inspect sparse operand storage");
-    if (!s.ok()) return s;
   }
   if (out) *out = b;
   return Status::Ok();

@@ -36,6 +36,9 @@ bool Overlap(Span a, Span b);
 
 // ValidateSparseMetadata + ValidateSparseDevice (operations.cc:134-276).
 Status ValidateSparse(const asc_sb_sparse& m, int device, SparseBytes* bytes);
+// The metadata half alone (format, kind, extents, trust, sizes, alignment,
+// overlap): no memory-space or pointer-attribute checks.
+Status ValidateSparseMetadata(const asc_sb_sparse& m, SparseBytes* bytes);
 // VectorBytes + ValidateVector (operations.cc:278-332).  `span` receives the
 // bytes actually touched by the vector (lowest to highest element).
 Status ValidateVector(const asc_sb_vector& v, int kind, bool writable,

@@ -162,18 +162,81 @@ class CudaCsrArray:
         return d
 
 
+def _host_sparse_desc(rows, columns, offsets, indices, values, fmt) -> _abi.SparseDesc:
+    d = _abi.SparseDesc()
+    pinned = isinstance(values, torch.Tensor) and values.is_pinned()
+    d.structure_first = _host_ptr(offsets)
+    d.structure_second = _host_ptr(indices) if len(indices) else None
+    d.values = _host_ptr(values) if len(values) else None
+    d.memory_space = MemorySpace.kPinnedHost if pinned else MemorySpace.kHost
+    d.element_kind = _kind(values.dtype if isinstance(values, torch.Tensor)
+                           else torch.from_numpy(values[:0]).dtype)
+    d.format = int(fmt)
+    d.canonical_structure_trusted = 1
+    d.rows, d.columns, d.nonzeros = rows, columns, len(values)
+    return d
+
+
+def _host_ptr(a) -> int:
+    return a.data_ptr() if isinstance(a, torch.Tensor) else a.ctypes.data
+
+
 def CudaCloneCsr(context: SparseCudaContext, rows: int, columns: int,
-                 offsets: np.ndarray, indices: np.ndarray, values: np.ndarray,
+                 offsets, indices, values,
                  fmt: FormatKind = FormatKind.kCsr) -> CudaCsrArray:
-    """Host CSR -> trusted device CSR (cuda.h:1040-1056).  The structure must
-    already be canonical (the reference validates it on the host first)."""
+    """Host CSR -> trusted device CSR (cuda.h:1040-1056) through
+    asc_sb_clone_csr: device arrays allocated here (the caller's resource in
+    the reference), copies on the context stream, pageable sources staged
+    through pinned buffers.  Arrays are numpy arrays or (pinned) CPU tensors;
+    the structure must already be canonical."""
+    if not isinstance(offsets, torch.Tensor):
+        offsets = np.ascontiguousarray(offsets, np.int64)
+        indices = np.ascontiguousarray(indices, np.int64)
+        values = np.ascontiguousarray(values)
     dev = torch.device("cuda", context.device)
-    with torch.cuda.stream(context.stream):
-        off = torch.from_numpy(np.ascontiguousarray(offsets, np.int64)).to(dev, non_blocking=False)
-        idx = torch.from_numpy(np.ascontiguousarray(indices, np.int64)).to(dev)
-        val = torch.from_numpy(np.ascontiguousarray(values)).to(dev)
-    context.stream.synchronize()
-    return CudaCsrArray(rows, columns, off, idx, val, fmt)
+    vdtype = values.dtype if isinstance(values, torch.Tensor) else \
+        torch.from_numpy(values[:0]).dtype
+    off = torch.empty(len(offsets), dtype=torch.int64, device=dev)
+    idx = torch.empty(len(indices), dtype=torch.int64, device=dev)
+    val = torch.empty(len(values), dtype=vdtype, device=dev)
+    out = CudaCsrArray(rows, columns, off, idx, val, fmt)
+    src = _host_sparse_desc(rows, columns, offsets, indices, values, fmt)
+    dst = out.describe()
+    context.check(context._lib.asc_sb_clone_csr(context.handle, ctypes.byref(src),
+                                                ctypes.byref(dst)))
+    return out
+
+
+def CudaCloneIndexedVector(context: SparseCudaContext, indices, values,
+                           dense_extent: int) -> tuple[torch.Tensor, torch.Tensor]:
+    """Host indexed vector -> device (CloneIndexedErased semantics):
+    returns the device (indices, values)."""
+    from ._abi import IndexedDesc
+    if not isinstance(indices, torch.Tensor):
+        indices = np.ascontiguousarray(indices, np.int64)
+        values = np.ascontiguousarray(values)
+    dev = torch.device("cuda", context.device)
+    vdtype = values.dtype if isinstance(values, torch.Tensor) else \
+        torch.from_numpy(values[:0]).dtype
+    d_idx = torch.empty(len(indices), dtype=torch.int64, device=dev)
+    d_val = torch.empty(len(values), dtype=vdtype, device=dev)
+    s, d = IndexedDesc(), IndexedDesc()
+    pinned = isinstance(values, torch.Tensor) and values.is_pinned()
+    s.indices = _host_ptr(indices) if len(indices) else None
+    s.values = _host_ptr(values) if len(values) else None
+    s.memory_space = MemorySpace.kPinnedHost if pinned else MemorySpace.kHost
+    d.indices = d_idx.data_ptr() if len(indices) else None
+    d.values = d_val.data_ptr() if len(values) else None
+    d.memory_space = MemorySpace.kDevice
+    for x in (s, d):
+        x.element_kind = _kind(vdtype)
+        x.nonzeros = len(values)
+        x.dense_extent = dense_extent
+        x.writable = 1
+        x.canonical_structure_trusted = 1
+    context.check(context._lib.asc_sb_clone_indexed(context.handle, ctypes.byref(s),
+                                                    ctypes.byref(d)))
+    return d_idx, d_val
 
 
 @dataclass

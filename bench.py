@@ -373,7 +373,7 @@ EXTRA = ("spmv_powerlaw_4M_f32", "spmv_t_powerlaw_4M_f64", "spmv_t_powerlaw_4M_f
          "spmm_block_k8", "spmm_block_k32", "spmm_block_k128", "batched_banded_4096",
          "sptrsv_laplacian_1M_f64", "sptrsv_stencil27_2M_f64", "sptrsv_powerlaw_4M_f64",
          "sptrsv_random_2M_f64", "sptrsv_random_2M_f32",
-         "level1_16M_f64")
+         "level1_16M_f64", "clone_powerlaw_4M_f64")
 
 
 def _timer(stream, steps, warmup):
@@ -549,6 +549,46 @@ def run_extra(args):
         dtype_s = "f32" if dt == np.float32 else "f64"
         extra_cfg.update({"rows": n, "nnz": a_h.nnz, "op": "none", "triangle": "lower",
                           "rhs_restore_ms_subtracted": round(copy_ms, 4)})
+    elif w.startswith("clone"):
+        # host -> device clone of the 4M-row power-law matrix (1.18 GB of CSR)
+        a_h = synthetic.power_law(4_194_304, 16.0, 1.5, 65_536, seed=1)
+        byts = a_h.ptr.nbytes + a_h.idx.nbytes + a_h.val.nbytes
+        ptr_p, idx_p, val_p = (torch.from_numpy(a).pin_memory() for a in (a_h.ptr, a_h.idx, a_h.val))
+        keep = []
+
+        def clone(pinned):
+            src = (ptr_p, idx_p, val_p) if pinned else (a_h.ptr, a_h.idx, a_h.val)
+            keep.append(sc.CudaCloneCsr(ctx, a_h.rows, a_h.cols, *src))
+            if len(keep) > 2:
+                keep.pop(0)
+
+        def torch_pageable():
+            keep.append(tuple(torch.from_numpy(a).to(dev) for a in (a_h.ptr, a_h.idx, a_h.val)))
+            if len(keep) > 2:
+                keep.pop(0)
+        for name, fn in (("clone_pageable", lambda: clone(False)),
+                         ("clone_pinned", lambda: clone(True)),
+                         ("torch_pageable_to_device", torch_pageable)):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                fn()
+            torch.cuda.synchronize()
+            ms = (time.perf_counter() - t0) * 1e3 / args.steps
+            detail[name] = {"ms": round(ms, 3), "gbs": round(byts / ms / 1e6, 2)}
+        dtype_s = "f64"
+        extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "bytes": byts,
+                          "timing": "host wall clock around each clone, synchronized"})
+        out = {"metric": "host-to-device clone GB/s", "value": detail["clone_pageable"]["gbs"],
+               "unit": "GB/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": detail["clone_pageable"]["ms"], "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": dtype_s, "data": "synthetic",
+               "config": {"workload": w, **extra_cfg}, "detail": detail}
+        ctx.close()
+        print(json.dumps(out), flush=True)
+        return 0
     elif w.startswith("level1"):
         from asc_cpp_b200._abi import Level1Op
         n, nnz = 64 * 1024 * 1024, 16 * 1024 * 1024

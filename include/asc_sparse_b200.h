@@ -306,6 +306,25 @@ ASC_SB_API int asc_sb_standard_triangular_solve(asc_sb_context* context, int32_t
                                                 int32_t triangle, int32_t diagonal,
                                                 const asc_sb_dense* right_hand_sides);
 
+/* ---- host -> device clones ------------------------------------------------
+ * Replace the copy half of internal_sparse_cuda::CloneCsrErased and
+ * CloneIndexedErased (cuda.h:212-219; operations.cc:696-880).  The caller
+ * allocates the destination arrays (in the reference the clone allocates them
+ * from the caller's MemoryResource) and describes them with the source's
+ * shape, kind and nonzero count in device memory.  The copies are enqueued on
+ * the context stream.  Pageable sources (ASC_SB_HOST) are staged through a
+ * context-owned pinned ring filled by host copy threads (created on first
+ * use): when the call returns, the source has been read completely.
+ * Page-locked sources are copied by DMA directly and must stay unchanged
+ * until the stream has passed the copy.  The source must be canonical
+ * (canonical_structure_trusted, as the reference's host views guarantee);
+ * the destination is then a trusted device array. */
+ASC_SB_API int asc_sb_clone_csr(asc_sb_context* context, const asc_sb_sparse* source,
+                                const asc_sb_sparse* destination);
+ASC_SB_API int asc_sb_clone_indexed(asc_sb_context* context,
+                                    const asc_sb_indexed_vector* source,
+                                    const asc_sb_indexed_vector* destination);
+
 /* ---- analysis plans (no reference counterpart) ----------------------------
  * A plan caches, in caller-provided device memory, everything the kernels can
  * reuse across calls on one matrix: the row-tile and merge-path partitions and
