@@ -44,6 +44,7 @@ struct SegSmem {
   int rowid[33];                   // k-th nonempty row of the tile -> lane
   int64_t bnd[kChunk + 1];         // first row of tiles c0 .. c0 + kChunk
   T yinit[33];                     // exact standard form: y of the k-th row
+  T prod[kItems];                  // exact form: products of a long row's tail
 };
 
 // Arithmetic of the two modes.  EXACT rounds every product and sum separately
@@ -295,29 +296,43 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
   const T carry_out = __shfl_sync(0xffffffffu, c, 31);
 
   if (!ends_here) {
-    // long last row: the nonzeros past the window
+    // long last row: the nonzeros past the window, 256 per round, each lane
+    // 8 contiguous ones with vector loads (the window ends on an aligned
+    // position: a0 + kItems, so every round starts aligned too)
     T total;
-    if (!EXACT) {
-      T part = T(0);
-      for (int64_t q = base + window + lane; q < base + span; q += 32) {
-        part = fma(ld_stream(val + q), ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)), part);
-      }
+    T part = T(0);
+    total = carry_out;
+    for (int64_t q0 = base + window; q0 < base + span; q0 += kItems) {
+      const int64_t rem = base + span - q0;
+      const int cnt = static_cast<int>(rem < kItems ? rem : kItems);
+      const int hi = cnt - p0 < 0 ? 0 : (cnt - p0 > kPer ? kPer : cnt - p0);
+      const uint32_t m = (1u << hi) - 1u;
+      T q[kPer];
+      lane_products<T, EXACT, STANDARD, UNIT>(q, m, idx + (q0 + p0), val + (q0 + p0), x, incx,
+                                              alpha);
+      if (!EXACT) {
 #pragma unroll
-      for (int m = 16; m > 0; m >>= 1) part += shfl_xor(part, m);
-      total = carry_out + part;
-    } else {
-      // 32 products per round, then added in stored order
-      total = carry_out;
-      for (int64_t q0 = base + window; q0 < base + span; q0 += 32) {
-        const int64_t q = q0 + lane;
-        T pv = T(0);
-        if (q < base + span) {
-          pv = product<true, STANDARD>(alpha, ld_stream(val + q),
-                                       ld_gather(&at<UNIT>(x, ld_stream(idx + q), incx)));
+        for (int k = 0; k < kPer; ++k) part += q[k];
+      } else {
+        // stored order: lane 0 adds the round's products from shared memory
+#pragma unroll
+        for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = q[k];
+        __syncwarp();
+        if (lane == 0) {
+          int k = 0;
+          for (; k + 8 <= cnt; k += 8) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) total = add_rn(total, w.prod[k + u]);
+          }
+          for (; k < cnt; ++k) total = add_rn(total, w.prod[k]);
         }
-        const int n = static_cast<int>(base + span - q0 < 32 ? base + span - q0 : 32);
-        for (int k = 0; k < n; ++k) total = add_rn(total, __shfl_sync(0xffffffffu, pv, k));
+        __syncwarp();
       }
+    }
+    if (!EXACT) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) part += shfl_xor(part, o);
+      total = carry_out + part;
     }
     if (lane == 0) {
       T* yp = &at<UNIT>(y, r0 + nr - 1, incy);

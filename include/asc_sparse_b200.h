@@ -264,7 +264,7 @@ enum { ASC_SB_L1_DOT = 0, ASC_SB_L1_AXPY = 1, ASC_SB_L1_GATHER = 2,
 /* asc::SparseBlasConjugation, blas.h:74-77 */
 enum { ASC_SB_UNCONJUGATED = 0, ASC_SB_CONJUGATED = 1 };
 
-/* Replaces internal_sparse_cuda::StandardLevel1Erased (cuda.h:228-233;
+/* Replaces internal_sparse_cuda::StandardLevel1Erased (cuda.h:234-238;
  * operations.cc:1122-1212), CPU contract blas.h:1340-1600:
  *   DOT          result[0] = sum_k v'_k x[i_k]  (v' = conj(v) if CONJUGATED)
  *   AXPY         x[i_k] += alpha v_k   (alpha == 0: nothing is touched)
