@@ -24,8 +24,9 @@
 // per output, n = stored entries in the row (tests check this bound).
 //
 // Pipeline: four producer warps each own one shared-memory stage and load,
-// split and store the blocks whose running index is their warp number mod 4,
-// so four blocks' loads are in flight per CTA; one thread issues the MMAs as
+// split and store the blocks whose running index is their warp number mod 4;
+// a warp issues the next block's loads before it waits for its stage, so up
+// to eight blocks' loads are in flight per CTA; one thread issues the MMAs as
 // stages fill (mbarriers full / empty); two 16-column accumulators alternate
 // between block rows so the epilogue of one overlaps the MMAs of the next.
 // Every wait is bounded: one that runs out records 1 in *status, tells the
@@ -235,10 +236,8 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
       const float* a1 = val + __ldg(ptr + br * kB + ar + 8) + ac * 4;
       for (int64_t j = 0; j < nblk; ++j, ++it) {
         if ((it & 3u) != static_cast<uint32_t>(p)) continue;
-        if (uses > 0 && !wait_bar(&s.empty[p], (uses - 1) & 1u, &s.abort)) {
-          failed = true;
-          break;
-        }
+        // the block's loads go out before the wait for the stage, so their
+        // latency overlaps the MMAs still reading it
         const int64_t bc = __ldg(idx + p0 + j * kB) >> 4;
         const float4 va0 = __ldg(reinterpret_cast<const float4*>(a0 + j * kB));
         const float4 va1 = __ldg(reinterpret_cast<const float4*>(a1 + j * kB));
@@ -251,6 +250,10 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
           for (int kk = 0; kk < kB; ++kk) {
             bv[i][kk] = m < width ? __ldg(brow + kk * ldb + m) : 0.0f;
           }
+        }
+        if (uses > 0 && !wait_bar(&s.empty[p], (uses - 1) & 1u, &s.abort)) {
+          failed = true;
+          break;
         }
         float4 hi, lo;
         split(va0, hi, lo);
