@@ -288,7 +288,7 @@ __device__ __forceinline__ unsigned long long take_ticket(Control* ctl, int lane
 // published values.  Lane 0 ends with the row's value.
 template <typename T, bool EXACT>
 __device__ void warp_row(const ascb_trsv& a, int64_t row, T alpha, T* pub, Control* ctl,
-                         int lane) {
+                         int lane, T* stage) {
   using A = Ar<T>;
   const T* __restrict__ val = static_cast<const T*>(a.val);
   T* x = static_cast<T*>(a.x);
@@ -323,12 +323,20 @@ __device__ void warp_row(const ascb_trsv& a, int64_t row, T alpha, T* pub, Contr
     const unsigned dmask = __ballot_sync(kFull, is_diag);
     if (dmask != 0u) diag = A::shfl(v, __ffs(dmask) - 1);
     if (EXACT) {
-      unsigned mask = __ballot_sync(kFull, dep);
-      while (mask != 0u) {
-        const int src = __ffs(mask) - 1;
-        mask &= mask - 1u;
-        const T pk = A::shfl(prod, src);
-        if (lane == 0) value = A::sub(value, pk);
+      // the chunk's dependencies are contiguous lanes (sorted columns): lane 0
+      // subtracts their products in stored order from shared memory
+      const unsigned mask = __ballot_sync(kFull, dep);
+      if (mask != 0u) {
+        stage[lane] = prod;
+        __syncwarp();
+        if (lane == 0) {
+          const int first = __ffs(mask) - 1;
+          const int last = 31 - __clz(mask);
+          for (int q = first; q <= last; ++q) {
+            if ((mask >> q) & 1u) value = A::sub(value, stage[q]);
+          }
+        }
+        __syncwarp();
       }
     }
   }
@@ -369,7 +377,8 @@ __global__ void __launch_bounds__(kThreads) trsv_single(ascb_trsv a, T alpha) {
     if (__any_sync(kFull, end - p > kLongRow)) {
       const int64_t count = a.n - s0 < 32 ? a.n - s0 : 32;
       for (int64_t i = 0; i < count; ++i) {
-        warp_row<T, EXACT>(a, __shfl_sync(kFull, row, static_cast<int>(i)), alpha, pub, ctl, lane);
+        warp_row<T, EXACT>(a, __shfl_sync(kFull, row, static_cast<int>(i)), alpha, pub, ctl, lane,
+                           solved_value[warp]);
       }
       continue;
     }
