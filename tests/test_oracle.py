@@ -393,3 +393,72 @@ def test_trsv_restatement_matches_reference_larger(restatement, reference):
             got = restatement.triangular_solve(op, triangle, 1, 300, m.ptr, m.idx, m.val, 1.0,
                                                b, 1, None, 2)
             assert _bits_equal(got, want)
+
+
+def test_trsv_edge_cases_against_reference(restatement, reference):
+    """Shapes at the edges of the solve, each through both the restatement
+    and the reference's own SparseTriangularSolveMultiple: a 1 x 1 system,
+    a diagonal-only matrix (empty strict triangle), alpha = 0 over NaN
+    entries (zeros without reading B), one and five right-hand sides with a
+    leading dimension larger than the matrix needs, all four kinds."""
+    rng = np.random.default_rng(91)
+    for dt in TRSV_TAGS.values():
+        cplx = np.iscomplexobj(dt(0))
+        one = (np.array([2.5 - 1j]) if cplx else np.array([2.5])).astype(dt)
+        cases = [(1, np.array([0, 1], np.int64), np.array([0], np.int64), one)]
+        d = synthetic._values(rng, 7, dt) + dt(3)
+        cases.append((7, np.arange(8, dtype=np.int64), np.arange(7, dtype=np.int64), d))
+        m = synthetic.triangular(rng, 30, lower=False, dtype=dt)
+        cases.append((30, m.ptr, m.idx, m.val))
+        for n, ptr, idx, val in cases:
+            for op in (0, 1, 2):
+                for triangle in (0, 1):
+                    for diagonal in (0, 1):
+                        if n == 30 and triangle == 1:
+                            continue  # the upper matrix is not lower triangular
+                        for layout, k, ld in ((1, 1, 1), (1, 5, 7), (0, 5, n + 3)):
+                            size = (n * ld) if layout == 1 else (k * ld)
+                            b = synthetic._values(rng, size, dt)
+                            alpha = (0.5 + 2j) if cplx else -0.75
+                            rc, want = reference.triangular_solve(op, triangle, diagonal, n, ptr,
+                                                                  idx, val, alpha, b, layout, ld,
+                                                                  k)
+                            assert rc == 0
+                            got = restatement.triangular_solve(op, triangle, diagonal, n, ptr,
+                                                               idx, val, alpha, b, layout, ld, k)
+                            if cplx and dt == np.complex64 and diagonal == 0:
+                                np.testing.assert_allclose(got, want, rtol=2e-5, atol=2e-6)
+                            else:
+                                assert _bits_equal(got, want), (n, op, triangle, diagonal, k)
+        # alpha = 0: zeros, whatever the matrix holds
+        nan_val = np.full(7, np.nan, dt)
+        b = synthetic._values(rng, 7, dt)
+        rc, want = reference.triangular_solve(0, 1, 1, 7, np.arange(8, dtype=np.int64),
+                                              np.arange(7, dtype=np.int64), nan_val, 0.0, b)
+        got = restatement.triangular_solve(0, 1, 1, 7, np.arange(8, dtype=np.int64),
+                                           np.arange(7, dtype=np.int64), nan_val, 0.0, b)
+        assert rc == 0 and _bits_equal(got, want) and not got.any()
+
+
+def test_triangular_generators_are_canonical():
+    """synthetic.triangular and triangle_of give canonical CSR (sorted,
+    unique columns per row) inside the requested triangle, diagonal included."""
+    rng = np.random.default_rng(5)
+    for lower in (True, False):
+        m = synthetic.triangular(rng, 5000, lower=lower, near=5, far=3, span=40)
+        rows = np.repeat(np.arange(m.rows), np.diff(m.ptr))
+        same_row = rows[1:] == rows[:-1]
+        assert (np.diff(m.idx)[same_row] > 0).all()
+        assert ((m.idx <= rows) if lower else (m.idx >= rows)).all()
+        diag = m.idx == rows
+        assert np.bincount(rows[diag], minlength=m.rows).tolist() == [1] * m.rows
+        off = np.bincount(rows[~diag], weights=np.abs(m.val[~diag]), minlength=m.rows)
+        assert (np.abs(m.val[diag]) >= off + 1 - 1e-12).all()  # diagonally dominant
+    lap = synthetic.laplacian_2d(20)
+    for lower in (True, False):
+        t = synthetic.triangle_of(lap, lower)
+        rows = np.repeat(np.arange(t.rows), np.diff(t.ptr))
+        assert ((t.idx <= rows) if lower else (t.idx >= rows)).all()
+        full_rows = np.repeat(np.arange(lap.rows), np.diff(lap.ptr))
+        keep = (lap.idx <= full_rows) if lower else (lap.idx >= full_rows)
+        assert _bits_equal(t.idx, lap.idx[keep]) and _bits_equal(t.val, lap.val[keep])
