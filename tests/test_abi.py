@@ -92,3 +92,47 @@ def test_enum_values_match_reference_numbering():
     assert _abi.SparseBlasTranspose.kConjugateTranspose == 2
     assert _abi.SparseBlasLayout.kRowMajor == 1
     assert _abi.Determinism.kBackendDefault == 1
+
+
+def test_null_arguments_return_error_codes(lib_path):
+    """Every entry point called with a null context and null descriptors
+    returns an error code (or, for the destroy calls, succeeds as a no-op)
+    instead of dereferencing anything: host logic, no device needed."""
+    from asc_cpp_b200 import _abi
+    lib = _abi.load()
+    no_op = {"asc_sb_context_destroy", "asc_sb_plan_destroy", "asc_sb_batch_destroy"}
+    for name, (restype, argtypes) in _abi.SIGNATURES.items():
+        args = []
+        for t in argtypes:
+            if t in (ctypes.c_double, ctypes.c_float):
+                args.append(t(0.0))
+            elif t in (ctypes.c_int32, ctypes.c_int64, ctypes.c_size_t):
+                args.append(t(0))
+            else:
+                args.append(None)
+        r = getattr(lib, name)(*args)
+        if name in no_op:
+            assert r == _abi.ErrorCode.kOk, name
+        elif name == "asc_sb_context_stream":
+            assert r is None
+        elif name == "asc_sb_context_last_error":
+            assert r  # a message, not a crash
+        elif name == "asc_sb_context_launch_count":
+            assert r == 0
+        elif name == "asc_sb_selector_param_count":
+            assert r < 0  # zero variants is not a network
+        else:
+            assert r in (_abi.ErrorCode.kInvalidArgument, _abi.ErrorCode.kInvalidState), (name, r)
+
+
+def test_context_without_a_device_is_unavailable(lib_path):
+    """On a host without a CUDA device the context cannot be created and the
+    call says so (ASC_SB_UNAVAILABLE) rather than failing later."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from asc_cpp_b200 import _abi
+    lib = _abi.load()
+    ctx = ctypes.c_void_p()
+    assert lib.asc_sb_context_create(0, None, ctypes.byref(ctx)) == _abi.ErrorCode.kUnavailable
+    assert not ctx.value
