@@ -462,3 +462,55 @@ def test_triangular_generators_are_canonical():
         full_rows = np.repeat(np.arange(lap.rows), np.diff(lap.ptr))
         keep = (lap.idx <= full_rows) if lower else (lap.idx >= full_rows)
         assert _bits_equal(t.idx, lap.idx[keep]) and _bits_equal(t.val, lap.val[keep])
+
+
+from hypothesis import HealthCheck, given, settings, strategies as st  # noqa: E402
+
+
+@st.composite
+def _small_csr(draw):
+    rows = draw(st.integers(0, 12))
+    cols = draw(st.integers(0, 12))
+    seed = draw(st.integers(0, 2**31 - 1))
+    rng = np.random.default_rng(seed)
+    lengths = rng.integers(0, cols + 1, size=rows) if cols else np.zeros(rows, np.int64)
+    ptr = np.zeros(rows + 1, np.int64)
+    np.cumsum(lengths, out=ptr[1:])
+    idx = np.concatenate([np.sort(rng.choice(cols, int(n), replace=False))
+                          for n in lengths]).astype(np.int64) if ptr[-1] else np.zeros(0, np.int64)
+    val = rng.standard_normal(int(ptr[-1]))
+    return rows, cols, ptr, idx, val
+
+
+@settings(max_examples=150, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(_small_csr())
+def test_conversion_restatement_matches_reference_on_random_shapes(restatement, reference, m):
+    """CSR -> CSC and back through the restatement equal the reference's
+    ConvertToCsc / ConvertToCsr on random small shapes, empty rows, columns
+    and matrices included."""
+    rows, cols, ptr, idx, val = m
+    got = restatement.convert_compressed(True, rows, cols, ptr, idx, val)
+    want = reference.convert_compressed(True, rows, cols, ptr, idx, val)
+    for g, w in zip(got, want):
+        assert _bits_equal(np.asarray(g, w.dtype), w)
+    back = restatement.convert_compressed(False, rows, cols, *got)
+    assert _bits_equal(back[0], ptr) and _bits_equal(np.asarray(back[1], np.int64), idx)
+    assert _bits_equal(np.asarray(back[2]), val)
+
+
+@settings(max_examples=120, deadline=None, suppress_health_check=[HealthCheck.too_slow])
+@given(st.integers(1, 24), st.integers(0, 2**31 - 1), st.sampled_from([0, 1, 2]),
+       st.sampled_from([0, 1]), st.sampled_from([0, 1]),
+       st.sampled_from([np.float64, np.float32, np.complex128]))
+def test_trsv_restatement_matches_reference_on_random_systems(restatement, reference, n, seed,
+                                                              op, triangle, diagonal, dt):
+    rng = np.random.default_rng(seed)
+    m = synthetic.triangular(rng, n, lower=triangle == 1, near=2, far=1, span=4, dtype=dt)
+    b = synthetic._values(rng, 2 * n, dt)
+    alpha = (1.5 - 0.5j) if np.iscomplexobj(dt(0)) else 1.5
+    rc, want = reference.triangular_solve(op, triangle, diagonal, n, m.ptr, m.idx, m.val, alpha,
+                                          b, 1, 2, 2)
+    assert rc == 0
+    got = restatement.triangular_solve(op, triangle, diagonal, n, m.ptr, m.idx, m.val, alpha, b,
+                                       1, 2, 2)
+    assert _bits_equal(got, want)
