@@ -210,6 +210,7 @@ int asc_sb_batch_workspace_size(asc_sb_context* context, int64_t count,
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (bytes == nullptr || count < 0 || (count > 0 && matrices == nullptr)) {
     return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "batch arguments are invalid"));
   }
@@ -225,6 +226,7 @@ int asc_sb_batch_create(asc_sb_context* context, int64_t count, const asc_sb_spa
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (out == nullptr || count < 0 ||
       (count > 0 && (matrices == nullptr || inputs == nullptr || outputs == nullptr))) {
     return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "batch arguments are invalid"));
@@ -347,6 +349,7 @@ int asc_sb_batch_set_schedule(asc_sb_context* context, asc_sb_batch* batch, int3
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (batch == nullptr || chunk_tiles < 1 || chunk_tiles > 4096 || ctas_per_sm < 0 ||
       ctas_per_sm > 32) {
     return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "batch schedule is out of range"));
@@ -370,6 +373,7 @@ int asc_sb_batch_spmv(asc_sb_context* context, asc_sb_batch* batch, double alpha
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (batch == nullptr) return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "null batch"));
   if (batch->device != v.device) {
     return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "batch and context devices differ"));
@@ -384,6 +388,7 @@ int asc_sb_batch_spmv_per_matrix(asc_sb_context* context, asc_sb_batch* batch, d
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (batch == nullptr) return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "null batch"));
   if (batch->device != v.device) {
     return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "batch and context devices differ"));
@@ -399,6 +404,7 @@ int asc_sb_batch_capture(asc_sb_context* context, asc_sb_batch* batch, double al
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (batch == nullptr) return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "null batch"));
   Guard guard(v.device);
   if (!guard.ok()) return Done(v, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
@@ -438,6 +444,7 @@ int asc_sb_batch_autotune(asc_sb_context* context, asc_sb_batch* batch, double a
   ContextView v;
   if (!ascb::host::ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(context, &v);  // determinism and stream as of the lock
   if (batch == nullptr || reps < 1) {
     return Done(v, Fail(ASC_SB_INVALID_ARGUMENT, "batch autotune arguments are invalid"));
   }

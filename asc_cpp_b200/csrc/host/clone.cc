@@ -270,6 +270,7 @@ int asc_sb_clone_csr(asc_sb_context* ctx, const asc_sb_sparse* source,
         v, Fail(ASC_SB_SHAPE, "CudaCloneCsr destination does not match the source"));
   }
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(ctx, &v);  // determinism and stream as of the lock
   ascb::host::DeviceScope scope(v.device);
   if (!scope.ok()) {
     return ascb::host::Finish(v, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
@@ -356,6 +357,7 @@ int asc_sb_clone_indexed(asc_sb_context* ctx, const asc_sb_indexed_vector* sourc
         v, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse CUDA descriptor storage spans cannot overlap"));
   }
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ascb::host::ViewContext(ctx, &v);  // determinism and stream as of the lock
   ascb::host::DeviceScope scope(v.device);
   if (!scope.ok()) {
     return ascb::host::Finish(v, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));

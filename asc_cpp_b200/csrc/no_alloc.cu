@@ -1,14 +1,14 @@
 // CSR SpMV that allocates nothing: asc_sb_csr_spmv_no_alloc.
 //
 // Some callers cannot allocate device memory at the point where they need a
-// sparse product: code running while a CUDA graph is being captured (where a
-// cudaMalloc is not allowed), plugin hosts whose memory is owned by their own
-// allocator and that forbid raw device allocations, and latency-critical loops
-// that must not take the implicit device synchronisation a cudaMalloc or
-// cudaFree may cause.  They also cannot always hand in a workspace.  This entry
-// point serves them: the only scratch memory it needs -- the row-tile
-// partition of the matrix -- lives in one file-scope device array that every
-// GPU holds from the moment this library is loaded until the process exits.
+// sparse product, and cannot hand in a workspace either: plugin hosts whose
+// device memory belongs to the host application's own allocator (which
+// forbids raw device allocations by plugins), and latency-critical loops that
+// must not take the implicit device synchronisation a cudaMalloc or cudaFree
+// may cause.  This entry point serves them: the only scratch memory it needs
+// -- the row-tile partition of the matrix -- lives in one file-scope device
+// array that every GPU holds from the moment this library is loaded until the
+// process exits.
 //
 // Limits and rules, stated for users:
 //   * the array holds kNoAllocMaxBounds int64 tile bounds (2 MiB per GPU); a
@@ -21,9 +21,13 @@
 //     ordering between them -- race on it and may compute wrong results;
 //   * the array keeps whatever the last call wrote; each call overwrites every
 //     entry it reads before reading it, so nothing needs clearing;
+//   * it always runs the default kernel (the variant forced on a context with
+//     asc_sb_context_set_variant does not apply), so its results equal
+//     asc_sb_csr_spmv's when the context's variant is AUTO;
 //   * the first call on each device looks up the array's device address
-//     (cudaGetSymbolAddress).  Make that first call before any stream
-//     capture starts on that device.
+//     (cudaGetSymbolAddress) and keeps it.  Make that first call before any
+//     stream capture starts on that device.  A cudaDeviceReset invalidates
+//     the kept address: the entry point must not be used after one.
 // It calls no cudaMalloc, cudaFree or allocating library routine.
 #include <cuda_runtime.h>
 
@@ -95,6 +99,7 @@ extern "C" ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, doub
   ContextView v;
   if (!ViewContext(context, &v)) return ASC_SB_INVALID_STATE;
   std::lock_guard<std::mutex> lock(*v.mutex);
+  ViewContext(context, &v);  // determinism and stream as of the lock
   Guard guard(v.device);
   if (!guard.ok()) return Done(v, ASC_SB_UNAVAILABLE, "CUDA device is unavailable");
   if (matrix == nullptr || input == nullptr || output == nullptr) {

@@ -92,7 +92,8 @@ enum {
   ASC_SB_VARIANT_VECTOR = 1,      /* 'lanes' threads per row, shuffle sums    */
   ASC_SB_VARIANT_WARP_TILES = 2,  /* warp row tiles, FMA, parallel long rows  */
   ASC_SB_VARIANT_MERGE_PATH = 3,  /* merge-path balanced tiles + carry fix-up */
-  ASC_SB_VARIANT_ROW_SPLIT = 4    /* vector rows + long rows split over CTAs  */
+  ASC_SB_VARIANT_ROW_SPLIT = 4    /* warp row tiles; long rows' tails split
+                                     into 256-entry chunks over many warps   */
 };
 
 /* ---- descriptors ---------------------------------------------------------- */
@@ -162,8 +163,14 @@ ASC_SB_API int asc_sb_context_create(int32_t device, void* stream,
 ASC_SB_API int asc_sb_context_destroy(asc_sb_context* context);
 ASC_SB_API int asc_sb_context_set_determinism(asc_sb_context* context,
                                               int32_t determinism);
-/* Forces one SpMV variant (for autotuning and tests).  `lanes` is the threads
- * per row of the VECTOR / ROW_SPLIT variants (1..32, power of two; 0 = auto). */
+/* Forces one SpMV variant (for autotuning and tests); BACKEND_DEFAULT only
+ * (DETERMINISTIC always runs the bit-exact kernels).  `lanes` (1..32, power
+ * of two; 0 = auto) is the threads per row of VECTOR, and for ROW_SPLIT the
+ * number of 256-entry rounds a row may run past its tile before its tail is
+ * split over other warps (0 = 4).  ROW_SPLIT needs a plan or the
+ * asc_sb_csr_spmv workspace for its chunk table; without one (the standard
+ * path without a plan) long rows run inline as in WARP_TILES.  Its partial
+ * sums are combined in a fixed order, so results repeat run to run. */
 ASC_SB_API int asc_sb_context_set_variant(asc_sb_context* context,
                                           int32_t variant, int32_t lanes);
 ASC_SB_API void* asc_sb_context_stream(const asc_sb_context* context);
@@ -203,17 +210,23 @@ ASC_SB_API int asc_sb_csr_spmv(asc_sb_context* context, double alpha,
                                int32_t workspace_space);
 
 /* Compat SpMV that allocates nothing and takes no workspace.  No counterpart
- * in the reference: it is for callers that cannot allocate device memory when
- * they need the product -- code running during CUDA graph capture, plugin
- * hosts that forbid device allocations outside their own allocator, and
- * latency-critical loops that must not risk the device synchronisation of a
- * cudaMalloc/cudaFree.  Same contract and results as asc_sb_csr_spmv with the
- * context's determinism.  Its only scratch, the row-tile partition, is a
- * static 2 MiB device array per GPU (held until the process exits): matrices
- * needing more than 262,144 tile bounds -- ceil((8*rows + nnz)/256) + 1 --
- * are rejected with ASC_SB_UNSUPPORTED.  All calls on a device share that
- * array: calls that overlap on the GPU race.  The first call on each device
- * looks up the array's address; make it before any stream capture. */
+ * in the reference.  It is for callers that cannot allocate device memory
+ * when they need the product and cannot hand in a workspace either: plugin
+ * hosts whose device memory belongs to the host application's own allocator,
+ * which forbids raw device allocations by plugins, and latency-critical loops
+ * that must not risk the implicit device synchronisation of cudaMalloc or
+ * cudaFree.  Same validation, error codes and arithmetic as asc_sb_csr_spmv
+ * with the context's determinism; it always runs the default kernel and
+ * ignores a variant forced with asc_sb_context_set_variant, so its results
+ * equal asc_sb_csr_spmv's when the context's variant is AUTO.  Its only
+ * scratch, the row-tile partition, is a static 2 MiB device array per GPU
+ * (held from library load until process exit): matrices needing more than
+ * 262,144 tile bounds -- ceil((8*rows + nnz)/256) + 1 -- are rejected with
+ * ASC_SB_UNSUPPORTED.  All calls on a device share that array: calls that
+ * overlap on the GPU race.  The first call on each device looks up the
+ * array's device address, once; make that first call before any stream
+ * capture starts on the device.  A cudaDeviceReset invalidates the address
+ * looked up; do not use this entry point after one in the same process. */
 ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, double alpha,
                                         const asc_sb_sparse* matrix,
                                         const asc_sb_vector* input, double beta,

@@ -1,7 +1,9 @@
 """asc_sb_csr_spmv_no_alloc: the SpMV entry point for callers that cannot
-allocate device memory (graph capture, allocator-owning plugin hosts,
-latency-critical loops).  Its partition scratch is a static device array, so
-it takes no workspace; its results must equal asc_sb_csr_spmv's.
+allocate device memory or hand in a workspace (plugin hosts whose device
+memory belongs to the host application's allocator, latency-critical loops
+that must not take a cudaMalloc/cudaFree synchronisation).  Its partition
+scratch is a static device array, so it takes no workspace; its results must
+equal asc_sb_csr_spmv's.
 
 This file is collected last on purpose: it touches process-wide state (the
 shared static scratch), so a stop at the first failure has run everything
