@@ -98,6 +98,28 @@ class SparseDesc(ctypes.Structure):
                 ("nonzeros", ctypes.c_int64)]
 
 
+class TensorDesc(ctypes.Structure):
+    """asc_sb_tensor: a sparse descriptor of any rank (pointwise evaluation)."""
+    _fields_ = [("structure_first", ctypes.c_void_p),
+                ("structure_second", ctypes.c_void_p),
+                ("values", ctypes.c_void_p),
+                ("memory_space", ctypes.c_int32),
+                ("element_kind", ctypes.c_int32),
+                ("format", ctypes.c_int32),
+                ("canonical_structure_trusted", ctypes.c_int32),
+                ("rank", ctypes.c_int64),
+                ("extents", ctypes.POINTER(ctypes.c_int64)),
+                ("nonzeros", ctypes.c_int64)]
+
+
+class OperandDesc(ctypes.Structure):
+    """asc_sb_operand: a view with the destination's structure, or a scalar."""
+    _fields_ = [("kind", ctypes.c_int32),
+                ("reserved", ctypes.c_int32),
+                ("view", TensorDesc),
+                ("scalar", ctypes.c_double)]
+
+
 class VectorDesc(ctypes.Structure):
     _fields_ = [("data", ctypes.c_void_p),
                 ("reachable_data", ctypes.c_void_p),
@@ -224,6 +246,12 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_convert_compressed": (ctypes.c_int, [_P, _SP, _SP, _P, _SZ]),
     "asc_sb_convert_coordinates": (ctypes.c_int, [_P, _P, _P, _I32, _I64, _I64, _I64, _SP,
                                                   _P, _SZ]),
+    "asc_sb_sparse_storage_bytes": (ctypes.c_int, [_P, _SP, ctypes.POINTER(_SZ),
+                                                   ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
+    "asc_sb_indexed_storage_bytes": (ctypes.c_int, [_P, ctypes.POINTER(IndexedDesc),
+                                                    ctypes.POINTER(_SZ), ctypes.POINTER(_SZ)]),
+    "asc_sb_evaluate": (ctypes.c_int, [_P, _I32, ctypes.POINTER(OperandDesc),
+                                       ctypes.POINTER(OperandDesc), ctypes.POINTER(TensorDesc)]),
 }
 
 _lib: ctypes.CDLL | None = None

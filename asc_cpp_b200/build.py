@@ -20,6 +20,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libasc_sparse_b200.so")
+# measurement-only kernels (bench.py's gather-floor workload), a library of their own
+PROBE_SRC = os.path.join(CSRC, "probe", "gather_floor.cu")
+PROBE_LIB = os.path.join(HERE, "libasc_gather_probe.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -74,7 +77,21 @@ def build(force: bool = False, verbose: bool = False, out: str | None = None,
             return _build(force, verbose, out)
         finally:
             BUILD, COMMON = saved
-    return _build(force, verbose, LIB)
+    lib = _build(force, verbose, LIB)
+    build_probe(force)
+    return lib
+
+
+def build_probe(force: bool = False) -> str:
+    """The gather-floor probe library (not part of the Sparse BLAS library)."""
+    if (not force and os.path.exists(PROBE_LIB) and
+            os.path.getmtime(PROBE_LIB) >= os.path.getmtime(PROBE_SRC)):
+        return PROBE_LIB
+    cmd = [NVCC] + COMMON + ARCH + ["-shared", PROBE_SRC, "-o", PROBE_LIB]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed for {PROBE_SRC}:\n{res.stdout}\n{res.stderr}")
+    return PROBE_LIB
 
 
 def _build(force: bool, verbose: bool, lib: str) -> str:

@@ -25,6 +25,23 @@ __device__ __forceinline__ int64_t ld_stream(const int64_t* p) {
   return static_cast<int64_t>(__ldcs(reinterpret_cast<const long long*>(p)));
 }
 
+// 32-byte streamed loads (sm_100: one request per lane for 4 int64 / 4
+// double / 8 float); the address must be 32-byte aligned.
+__device__ __forceinline__ void ld_stream32(const int64_t* p, int64_t* o) {
+  asm volatile("ld.global.cs.v4.s64 {%0, %1, %2, %3}, [%4];"
+               : "=l"(o[0]), "=l"(o[1]), "=l"(o[2]), "=l"(o[3]) : "l"(p));
+}
+__device__ __forceinline__ void ld_stream32(const double* p, double* o) {
+  asm volatile("ld.global.cs.v4.f64 {%0, %1, %2, %3}, [%4];"
+               : "=d"(o[0]), "=d"(o[1]), "=d"(o[2]), "=d"(o[3]) : "l"(p));
+}
+__device__ __forceinline__ void ld_stream32(const float* p, float* o) {
+  asm volatile("ld.global.cs.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=f"(o[0]), "=f"(o[1]), "=f"(o[2]), "=f"(o[3]), "=f"(o[4]), "=f"(o[5]),
+                 "=f"(o[6]), "=f"(o[7])
+               : "l"(p));
+}
+
 // Gathered operand (x): read-only path, cached in L1 and L2.
 #ifndef ASCB_GATHER_NOALLOC
 template <typename T>

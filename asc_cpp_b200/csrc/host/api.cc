@@ -60,6 +60,7 @@ struct Partitions {
   std::int64_t n_warp = 0;
   const std::int64_t* merge_bounds = nullptr;  // ascb_merge_bounds pairs
   std::int64_t n_merge = 0;
+  void* split = nullptr;  // row-split block (ascb_split_bytes(nnz, 256) bytes)
 };
 
 struct asc_sb_plan {
@@ -189,10 +190,21 @@ std::size_t MergeBoundBytes(std::int64_t rows, std::int64_t nnz) {
 // The size is a function of the matrix shape only, so it is stable for a given
 // (A, x, y) (the reference's rule, operations.cc:884-909): room for the
 // partition of whichever kernel the context selects.
+// Row-split block of a structure with `nnz` entries, sized for the smallest
+// split threshold (tails longer than 256 positions), so one block serves
+// every threshold.
+std::size_t SplitBlockBytes(std::int64_t nnz) {
+  return RoundUp(ascb_split_bytes(nnz, 256), 256);
+}
 std::size_t CompatWorkspaceBytes(const asc_sb_sparse& m) {
   if (m.rows == 0 || m.columns == 0) return 0;
-  return std::max(WarpTileBytes(m.rows, m.nonzeros), MergeBoundBytes(m.rows, m.nonzeros));
+  return std::max(WarpTileBytes(m.rows, m.nonzeros) + SplitBlockBytes(m.nonzeros),
+                  MergeBoundBytes(m.rows, m.nonzeros));
 }
+
+// ROW_SPLIT: a row is split when its tail past the tile window exceeds this
+// many 256-position rounds (the context's or plan's "lanes" value overrides).
+constexpr std::int64_t kSplitRounds = 4;
 
 // Choice of SpMV kernel for a real CSR product.
 struct Choice {
@@ -278,6 +290,24 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
   const bool seg_aligned =
       ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
        static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
+  if (choice.variant == ASC_SB_VARIANT_ROW_SPLIT && seg_aligned) {
+    // the split block lives in the plan, or after the tile bounds in the
+    // caller's workspace; without either (the standard path without a plan)
+    // the row runs inline, as in WARP_TILES
+    void* block = planned != nullptr ? planned->split
+                  : scratch != nullptr
+                      ? static_cast<void*>(reinterpret_cast<unsigned char*>(scratch) +
+                                           WarpTileBytes(a.rows, a.nnz))
+                      : nullptr;
+    if (block != nullptr) {
+      const std::int64_t rounds = choice.lanes > 0 ? choice.lanes : kSplitRounds;
+      return Launched(ctx,
+                      ascb_spmv_split(ctx->stream, dtype, form, &a, alpha, beta, &x, &y,
+                                      tiles_ptr, tiles, rounds * ascb_warp_tile_items(), block,
+                                      ctx->sm_count),
+                      "CUDA could not launch the row-split SpMV kernels");
+    }
+  }
   if (seg_aligned) {
     return Launched(ctx,
                     ascb_spmv_seg(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
@@ -299,6 +329,7 @@ Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* bu
   auto* merge = reinterpret_cast<std::int64_t*>(buffer + WarpTileBytes(a.rows, a.nnz));
   out->warp_tiles = warp;
   out->merge_bounds = merge;
+  out->split = buffer + WarpTileBytes(a.rows, a.nnz) + MergeBoundBytes(a.rows, a.nnz);
   if (a.rows == 0) return Status::Ok();
   Status s = Launched(ctx,
                       ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
@@ -309,7 +340,7 @@ Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* bu
                   "CUDA could not launch the merge partition kernel");
 }
 std::size_t PartitionBytes(std::int64_t rows, std::int64_t nnz) {
-  return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz);
+  return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz) + SplitBlockBytes(nnz);
 }
 
 std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
@@ -450,7 +481,7 @@ bool ValidVariant(int variant, int lanes) {
     return lanes >= 1 && lanes <= 32 && (lanes & (lanes - 1)) == 0;
   }
   return variant == ASC_SB_VARIANT_ROW_ORDERED || variant == ASC_SB_VARIANT_WARP_TILES ||
-         variant == ASC_SB_VARIANT_MERGE_PATH;
+         variant == ASC_SB_VARIANT_MERGE_PATH || variant == ASC_SB_VARIANT_ROW_SPLIT;
 }
 
 struct CompatOperands {
@@ -584,9 +615,6 @@ int asc_sb_context_set_variant(asc_sb_context* ctx, int32_t variant, int32_t lan
   const bool lanes_ok = lanes == 0 || (lanes > 0 && lanes <= 32 && (lanes & (lanes - 1)) == 0);
   if (variant < ASC_SB_VARIANT_AUTO || variant > ASC_SB_VARIANT_ROW_SPLIT || !lanes_ok) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "Unknown SpMV variant or lane count"));
-  }
-  if (variant == ASC_SB_VARIANT_ROW_SPLIT) {
-    return Finish(ctx, Fail(ASC_SB_UNSUPPORTED, "This SpMV variant is not available yet"));
   }
   std::lock_guard<std::mutex> lock(ctx->mutex);
   ctx->variant = variant;

@@ -374,4 +374,45 @@ int asc_sb_clone_indexed(asc_sb_context* ctx, const asc_sb_indexed_vector* sourc
   return ascb::host::Finish(v, ascb::host::CopyAll(v, items));
 }
 
+int asc_sb_sparse_storage_bytes(asc_sb_context* ctx, const asc_sb_sparse* source,
+                                size_t* offsets, size_t* indices, size_t* values) {
+  ContextView v;
+  if (!ascb::host::ViewContext(ctx, &v)) return ASC_SB_INVALID_STATE;
+  if (source == nullptr || offsets == nullptr || indices == nullptr || values == nullptr) {
+    return ascb::host::Finish(v, Fail(ASC_SB_INVALID_ARGUMENT, "storage arguments cannot be null"));
+  }
+  SparseBytes sb;
+  Status s = ascb::host::ValidateSparseMetadata(*source, &sb);
+  if (!s.ok()) return ascb::host::Finish(v, s);
+  *offsets = sb.first;
+  *indices = sb.second;
+  *values = sb.values;
+  return ascb::host::Finish(v, Status::Ok());
+}
+
+int asc_sb_indexed_storage_bytes(asc_sb_context* ctx, const asc_sb_indexed_vector* source,
+                                 size_t* indices, size_t* values) {
+  ContextView v;
+  if (!ascb::host::ViewContext(ctx, &v)) return ASC_SB_INVALID_STATE;
+  if (source == nullptr || indices == nullptr || values == nullptr) {
+    return ascb::host::Finish(v, Fail(ASC_SB_INVALID_ARGUMENT, "storage arguments cannot be null"));
+  }
+  // ValidateIndexedMetadata (operations.cc:542-570)
+  if (source->nonzeros < 0 || source->dense_extent < 0 ||
+      source->nonzeros > source->dense_extent || !source->canonical_structure_trusted) {
+    return ascb::host::Finish(
+        v, Fail(ASC_SB_INVALID_ARGUMENT, "CUDA Sparse BLAS requires a canonical indexed vector"));
+  }
+  if (source->element_kind < ASC_SB_FLOAT || source->element_kind > ASC_SB_COMPLEX_DOUBLE) {
+    return ascb::host::Finish(v, Fail(ASC_SB_INVALID_ARGUMENT, "Sparse CUDA scalar kind is invalid"));
+  }
+  const std::size_t n = static_cast<std::size_t>(source->nonzeros);
+  if (n > SIZE_MAX / 16) {
+    return ascb::host::Finish(v, Fail(ASC_SB_OVERFLOW, "Sparse CUDA storage size overflows"));
+  }
+  *indices = n * 8;
+  *values = n * ascb::host::ElementBytes(source->element_kind);
+  return ascb::host::Finish(v, Status::Ok());
+}
+
 }  // extern "C"

@@ -85,6 +85,16 @@ int ascb_spmv_seg_alignment(void);
 int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
                   double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
                   int64_t ntiles, int sm_count);
+// Row split (contracted only): like ascb_spmv_seg with exact = 0, except that
+// a row running more than split_min (>= 256) positions past its tile's window
+// is finished by a second kernel whose warps take its tail in 256-position
+// chunks; partial sums are combined in chunk order, so results repeat run to
+// run.  `block`: ascb_split_bytes(nnz, split_min) device bytes, 256-byte
+// aligned (its control words are cleared on the stream by the call).
+size_t ascb_split_bytes(int64_t nnz, int64_t split_min);
+int ascb_spmv_split(void* stream, int dtype, int form, const ascb_csr* a, double alpha,
+                    double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
+                    int64_t ntiles, int64_t split_min, void* block, int sm_count);
 // ---- batched compat SpMV: many independent CSR matrices, one launch ----
 // One matrix of a batch, as the persistent kernel reads it (device table).
 typedef struct ascb_batch_item {

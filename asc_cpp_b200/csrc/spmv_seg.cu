@@ -38,6 +38,31 @@ constexpr int kMaxDevices = 64;
 #define ASCB_SEG_MIN_CTAS 6
 #endif
 
+// Row split (BACKEND_DEFAULT): a tile whose last row runs more than
+// `split_min` positions past the tile's window does not walk that tail
+// itself.  It reserves an entry {row, first tail position, end, first chunk}
+// and stores the row's sum up to the window end as the entry's head; the
+// split kernel's warps then take the tail in 256-position chunks, each
+// writing one partial, and the warp that completes an entry's last chunk adds
+// head + partials in chunk order (a fixed tree), so results repeat run to run.
+struct SplitEntry {
+  int64_t row;    // < 0: not split (over capacity; never the case within bounds)
+  int64_t start;  // first tail position (16-byte aligned: the window end)
+  int64_t end;    // one past the row's last position
+  int64_t chunk;  // first chunk of this entry
+};
+struct SplitBlock {
+  unsigned long long* packed;  // (entries << 40) | chunks reserved; zero at launch
+  int* done;                   // chunks finished per entry; zero at launch
+  SplitEntry* entries;
+  void* head;                  // per entry, T
+  void* partial;               // per chunk, T
+  int64_t max_entries;
+  int64_t max_chunks;
+  int64_t split_min;
+};
+constexpr unsigned long long kChunkMask = (1ull << 40) - 1;
+
 template <typename T>
 struct SegSmem {
   uint32_t bits[kItems / 32 + 1];  // row-start bitmap of positions 0..256
@@ -95,45 +120,79 @@ __device__ __forceinline__ T finish(T s, T alpha, T beta, const T* yp) {
 // aligned); bit k of vmask says whether position k holds a nonzero of the
 // window.  Invalid positions give 0.  16-byte chunks that are wholly valid are
 // fetched with one vector load, others element by element.
-template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool V32 = false>
 __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
                                               const int64_t* __restrict__ ip,
                                               const T* __restrict__ vp, const T* __restrict__ x,
                                               int64_t incx, T alpha) {
   int64_t c[kPer];
   T v[kPer];
+  if constexpr (V32) {
+    // 32-byte aligned: one request per 32 bytes, so each sector a lane reads
+    // is touched once (16-byte loads touch every sector of a lane's run twice)
 #pragma unroll
-  for (int k = 0; k < kPer; k += 2) {
-    if (((vmask >> k) & 3u) == 3u) {
-      load_idx2(ip + k, c[k], c[k + 1]);
-    } else {
-      c[k] = ((vmask >> k) & 1u) ? ld_stream(ip + k) : 0;
-      c[k + 1] = ((vmask >> (k + 1)) & 1u) ? ld_stream(ip + k + 1) : 0;
-    }
-  }
-  if constexpr (sizeof(T) == 8) {
-#pragma unroll
-    for (int k = 0; k < kPer; k += 2) {
-      if (((vmask >> k) & 3u) == 3u) {
-        load_vec2(vp + k, v[k], v[k + 1]);
+    for (int k = 0; k < kPer; k += 4) {
+      if (((vmask >> k) & 15u) == 15u) {
+        ld_stream32(ip + k, c + k);
       } else {
-        v[k] = ((vmask >> k) & 1u) ? ld_stream(vp + k) : T(0);
-        v[k + 1] = ((vmask >> (k + 1)) & 1u) ? ld_stream(vp + k + 1) : T(0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) c[k + u] = ((vmask >> (k + u)) & 1u) ? ld_stream(ip + k + u) : 0;
+      }
+    }
+    if constexpr (sizeof(T) == 8) {
+#pragma unroll
+      for (int k = 0; k < kPer; k += 4) {
+        if (((vmask >> k) & 15u) == 15u) {
+          ld_stream32(vp + k, v + k);
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            v[k + u] = ((vmask >> (k + u)) & 1u) ? ld_stream(vp + k + u) : T(0);
+          }
+        }
+      }
+    } else {
+      if (vmask == 0xffu) {
+        ld_stream32(vp, v);
+      } else {
+#pragma unroll
+        for (int u = 0; u < kPer; ++u) v[u] = ((vmask >> u) & 1u) ? ld_stream(vp + u) : T(0);
       }
     }
   } else {
 #pragma unroll
-    for (int k = 0; k < kPer; k += 4) {
-      if (((vmask >> k) & 15u) == 15u) {
-        const float4 f = __ldcs(reinterpret_cast<const float4*>(vp + k));
-        v[k] = f.x;
-        v[k + 1] = f.y;
-        v[k + 2] = f.z;
-        v[k + 3] = f.w;
+    for (int k = 0; k < kPer; k += 2) {
+      if (((vmask >> k) & 3u) == 3u) {
+        load_idx2(ip + k, c[k], c[k + 1]);
       } else {
+        c[k] = ((vmask >> k) & 1u) ? ld_stream(ip + k) : 0;
+        c[k + 1] = ((vmask >> (k + 1)) & 1u) ? ld_stream(ip + k + 1) : 0;
+      }
+    }
+    if constexpr (sizeof(T) == 8) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          v[k + u] = ((vmask >> (k + u)) & 1u) ? ld_stream(vp + k + u) : T(0);
+      for (int k = 0; k < kPer; k += 2) {
+        if (((vmask >> k) & 3u) == 3u) {
+          load_vec2(vp + k, v[k], v[k + 1]);
+        } else {
+          v[k] = ((vmask >> k) & 1u) ? ld_stream(vp + k) : T(0);
+          v[k + 1] = ((vmask >> (k + 1)) & 1u) ? ld_stream(vp + k + 1) : T(0);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < kPer; k += 4) {
+        if (((vmask >> k) & 15u) == 15u) {
+          const float4 f = __ldcs(reinterpret_cast<const float4*>(vp + k));
+          v[k] = f.x;
+          v[k + 1] = f.y;
+          v[k + 2] = f.z;
+          v[k + 3] = f.w;
+        } else {
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            v[k + u] = ((vmask >> (k + u)) & 1u) ? ld_stream(vp + k + u) : T(0);
+          }
         }
       }
     }
@@ -149,15 +208,17 @@ __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
 // One tile: rows r0 .. r0 + nr - 1 (nr >= 1), whose ptr entries lane k holds
 // as rb = ptr[r0 + k], re = ptr[r0 + k + 1] (k < nr).  Shared by the
 // single-matrix and the batched kernels.
-template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false>
 __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t* __restrict__ idx,
                                          const T* __restrict__ val, const T* __restrict__ x,
                                          int64_t incx, T* __restrict__ y, int64_t incy, T alpha,
-                                         T beta, int64_t r0, int nr, int64_t rb, int64_t re) {
+                                         T beta, int64_t r0, int nr, int64_t rb, int64_t re,
+                                         const SplitBlock* split = nullptr) {
   const unsigned lt_mask = (1u << lane) - 1u;
   // window start alignment: each lane's 8 values and 8 indices start on a
-  // 16-byte boundary (arrays are 16-byte aligned, checked by the host)
-  constexpr int64_t kAlign = sizeof(T) == 8 ? 2 : 4;
+  // 16-byte (V32: 32-byte) boundary (the arrays are aligned so, checked by
+  // the host)
+  constexpr int64_t kAlign = V32 ? (sizeof(T) == 8 ? 4 : 8) : (sizeof(T) == 8 ? 2 : 4);
 
   const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
   const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
@@ -195,7 +256,7 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
   const int vhi = lim - p0 < 0 ? 0 : (lim - p0 > kPer ? kPer : lim - p0);
   const uint32_t vmask = ((1u << vhi) - 1u) & ~((1u << vlo) - 1u);
   T p[kPer];
-  lane_products<T, EXACT, STANDARD, UNIT>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
+  lane_products<T, EXACT, STANDARD, UNIT, V32>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
                                           alpha);
   const uint32_t word = w.bits[lane >> 2];
   const uint32_t flags = (word >> ((lane & 3) * 8)) & 0xffu;
@@ -295,6 +356,31 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
   }
   const T carry_out = __shfl_sync(0xffffffffu, c, 31);
 
+  if constexpr (SPLIT) {
+    if (!ends_here && span - window > split->split_min) {
+      // hand the tail to the split kernel: reserve an entry and its chunks
+      int64_t e = -1;
+      if (lane == 0) {
+        const int64_t tail = span - window;
+        const unsigned long long chunks =
+            static_cast<unsigned long long>((tail + kItems - 1) / kItems);
+        const unsigned long long old = atomicAdd(split->packed, (1ull << 40) | chunks);
+        const int64_t entry = static_cast<int64_t>(old >> 40);
+        const int64_t first = static_cast<int64_t>(old & kChunkMask);
+        if (entry < split->max_entries) {
+          const bool fits = first + static_cast<int64_t>(chunks) <= split->max_chunks;
+          split->entries[entry] = {fits ? r0 + nr - 1 : -1, base + window, base + span, first};
+          static_cast<T*>(split->head)[entry] = carry_out;
+          if (fits) e = entry;
+        }
+      }
+      e = __shfl_sync(0xffffffffu, e, 0);
+      if (e >= 0) {
+        __syncwarp();
+        return;
+      }
+    }
+  }
   if (!ends_here) {
     // long last row: the nonzeros past the window, 256 per round, each lane
     // 8 contiguous ones with vector loads (the window ends on an aligned
@@ -308,7 +394,7 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
       const int hi = cnt - p0 < 0 ? 0 : (cnt - p0 > kPer ? kPer : cnt - p0);
       const uint32_t m = (1u << hi) - 1u;
       T q[kPer];
-      lane_products<T, EXACT, STANDARD, UNIT>(q, m, idx + (q0 + p0), val + (q0 + p0), x, incx,
+      lane_products<T, EXACT, STANDARD, UNIT, V32>(q, m, idx + (q0 + p0), val + (q0 + p0), x, incx,
                                               alpha);
       if (!EXACT) {
 #pragma unroll
@@ -342,12 +428,12 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
   __syncwarp();  // bitmap and row tables are rewritten by the next tile
 }
 
-template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false>
 __global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
 seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
            const T* __restrict__ val, const T* __restrict__ x, int64_t incx, T* __restrict__ y,
            int64_t incy, T alpha, T beta, const int64_t* __restrict__ tile_row, int64_t ntiles,
-           int64_t rows, int64_t nnz) {
+           int64_t rows, int64_t nnz, SplitBlock split) {
   __shared__ SegSmem<T> smem_all[kWarpsPerCta];
   const int lane = threadIdx.x & 31;
   SegSmem<T>& w = smem_all[threadIdx.x >> 5];
@@ -397,10 +483,79 @@ seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
       re_n = lane < nr_n ? __ldg(ptr + r0_n + lane + 1) : 0;
     }
     if (nr == 0) continue;
-    seg_tile<T, EXACT, STANDARD, UNIT>(w, lane, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
-                                      rb, re);
+    seg_tile<T, EXACT, STANDARD, UNIT, SPLIT, V32>(w, lane, idx, val, x, incx, y, incy, alpha,
+                                                  beta, r0, nr, rb, re, &split);
   }
   (void)nnz;
+}
+
+// Tails of the split rows: warp-strided over the reserved chunks.  Chunk c of
+// entry e covers positions [start + 256 (c - chunk), ...) of its row; the
+// warp that finishes an entry's last chunk writes y.
+template <typename T, bool STANDARD, bool UNIT, bool V32>
+__global__ void __launch_bounds__(kThreads)
+split_chunk_kernel(const int64_t* __restrict__ idx, const T* __restrict__ val,
+                   const T* __restrict__ x, int64_t incx, T* __restrict__ y, int64_t incy,
+                   T alpha, T beta, SplitBlock split) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long packed = __ldcg(split.packed);
+  const int64_t entries = min(static_cast<int64_t>(packed >> 40), split.max_entries);
+  const int64_t chunks = min(static_cast<int64_t>(packed & kChunkMask), split.max_chunks);
+  const int64_t warp_id = static_cast<int64_t>(blockIdx.x) * kWarpsPerCta + (threadIdx.x >> 5);
+  const int64_t warp_count = static_cast<int64_t>(gridDim.x) * kWarpsPerCta;
+  const T* head = static_cast<const T*>(split.head);
+  T* partial = static_cast<T*>(split.partial);
+  const int p0 = kPer * lane;
+  for (int64_t c = warp_id; c < chunks; c += warp_count) {
+    // entry of chunk c: the last one whose first chunk is <= c (entries are
+    // reserved in increasing chunk order)
+    int64_t lo = 0, hi = entries - 1;
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (__ldcg(&split.entries[mid].chunk) <= c) {
+        lo = mid;
+      } else {
+        hi = mid - 1;
+      }
+    }
+    const int64_t row = __ldcg(&split.entries[lo].row);
+    if (row < 0) continue;
+    const int64_t start = __ldcg(&split.entries[lo].start);
+    const int64_t end = __ldcg(&split.entries[lo].end);
+    const int64_t first = __ldcg(&split.entries[lo].chunk);
+    const int64_t n_chunks = (end - start + kItems - 1) / kItems;
+    const int64_t q0 = start + (c - first) * kItems;
+    const int64_t rem = end - q0;
+    const int cnt = static_cast<int>(rem < kItems ? rem : kItems);
+    const int hiv = cnt - p0 < 0 ? 0 : (cnt - p0 > kPer ? kPer : cnt - p0);
+    T q[kPer];
+    lane_products<T, false, STANDARD, UNIT, V32>(q, (1u << hiv) - 1u, idx + (q0 + p0),
+                                                 val + (q0 + p0), x, incx, alpha);
+    T part = T(0);
+#pragma unroll
+    for (int k = 0; k < kPer; ++k) part += q[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += shfl_xor(part, o);
+    int finished = 0;
+    if (lane == 0) {
+      partial[c] = part;
+      __threadfence();
+      finished = atomicAdd(split.done + lo, 1) == n_chunks - 1;
+    }
+    finished = __shfl_sync(0xffffffffu, finished, 0);
+    if (finished) {
+      __threadfence();
+      // head + partials in a fixed order: lane l adds chunks l, l + 32, ...
+      T s = T(0);
+      for (int64_t j = lane; j < n_chunks; j += 32) s += __ldcg(partial + first + j);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += shfl_xor(s, o);
+      if (lane == 0) {
+        T* yp = &at<UNIT>(y, row, incy);
+        *yp = finish<false, STANDARD>(__ldcg(head + lo) + s, alpha, beta, yp);
+      }
+    }
+  }
 }
 
 // ---- batched: many independent matrices in one persistent launch ---------
@@ -512,20 +667,70 @@ int resident(Kernel kernel) {
   return cached[device];
 }
 
-template <typename T, bool EXACT, bool STANDARD, bool UNIT>
-int launch(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
-           const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count) {
-  auto kernel = seg_kernel<T, EXACT, STANDARD, UNIT>;
+// 32-byte loads when both streamed arrays start on 32-byte boundaries.
+inline bool aligned32(const ascb_csr* a) {
+  return ((reinterpret_cast<uintptr_t>(a->idx) | reinterpret_cast<uintptr_t>(a->val)) & 31u) == 0;
+}
+
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool V32>
+int launch_v(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
+             const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count) {
+  auto kernel = seg_kernel<T, EXACT, STANDARD, UNIT, false, V32>;
   const int64_t warps_needed = (ntiles + 3) / 4;
   const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
-  const int64_t resident_ctas =
-      static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * resident<T, EXACT, STANDARD, UNIT>(kernel);
+  const int64_t resident_ctas = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) *
+                                resident<T, EXACT, STANDARD, UNIT, V32 ? 4 : 0>(kernel);
   const unsigned blocks = static_cast<unsigned>(
       ctas_needed < 1 ? 1 : (ctas_needed < resident_ctas ? ctas_needed : resident_ctas));
   kernel<<<blocks, kThreads, 0, stream>>>(
       a->ptr, a->idx, static_cast<const T*>(a->val), static_cast<const T*>(x->data), x->stride,
-      static_cast<T*>(y->data), y->stride, alpha, beta, tile_row, ntiles, a->rows, a->nnz);
+      static_cast<T*>(y->data), y->stride, alpha, beta, tile_row, ntiles, a->rows, a->nnz,
+      SplitBlock{});
   return static_cast<int>(cudaGetLastError());
+}
+
+template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+int launch(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
+           const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count) {
+  return aligned32(a)
+             ? launch_v<T, EXACT, STANDARD, UNIT, true>(stream, a, alpha, beta, x, y, tile_row,
+                                                       ntiles, sm_count)
+             : launch_v<T, EXACT, STANDARD, UNIT, false>(stream, a, alpha, beta, x, y, tile_row,
+                                                        ntiles, sm_count);
+}
+
+template <typename T, bool STANDARD, bool UNIT, bool V32>
+int launch_split_v(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
+                   const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count,
+                   const SplitBlock& split) {
+  auto kernel = seg_kernel<T, false, STANDARD, UNIT, true, V32>;
+  const int64_t warps_needed = (ntiles + 3) / 4;
+  const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
+  const int per_sm = resident<T, false, STANDARD, UNIT, V32 ? 5 : 2>(kernel);
+  const int64_t resident_ctas = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * per_sm;
+  const unsigned blocks = static_cast<unsigned>(
+      ctas_needed < 1 ? 1 : (ctas_needed < resident_ctas ? ctas_needed : resident_ctas));
+  kernel<<<blocks, kThreads, 0, stream>>>(
+      a->ptr, a->idx, static_cast<const T*>(a->val), static_cast<const T*>(x->data), x->stride,
+      static_cast<T*>(y->data), y->stride, alpha, beta, tile_row, ntiles, a->rows, a->nnz, split);
+  int rc = static_cast<int>(cudaGetLastError());
+  if (rc != 0) return rc;
+  auto tails = split_chunk_kernel<T, STANDARD, UNIT, V32>;
+  const int tail_per_sm = resident<T, false, STANDARD, UNIT, V32 ? 6 : 3>(tails);
+  tails<<<static_cast<unsigned>((sm_count > 0 ? sm_count : 148) * tail_per_sm), kThreads, 0,
+          stream>>>(a->idx, static_cast<const T*>(a->val), static_cast<const T*>(x->data),
+                    x->stride, static_cast<T*>(y->data), y->stride, alpha, beta, split);
+  return static_cast<int>(cudaGetLastError());
+}
+
+template <typename T, bool STANDARD, bool UNIT>
+int launch_split(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
+                 const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count,
+                 const SplitBlock& split) {
+  return aligned32(a) ? launch_split_v<T, STANDARD, UNIT, true>(stream, a, alpha, beta, x, y,
+                                                                tile_row, ntiles, sm_count, split)
+                      : launch_split_v<T, STANDARD, UNIT, false>(stream, a, alpha, beta, x, y,
+                                                                 tile_row, ntiles, sm_count, split);
 }
 
 template <typename T, bool EXACT>
@@ -558,6 +763,78 @@ extern "C" int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const
 }
 
 extern "C" int ascb_spmv_seg_alignment(void) { return 16; }
+
+namespace ascb {
+namespace {
+
+// Layout of a row-split block for `nnz` stored entries and tails longer than
+// `split_min` (>= 256) positions: every split row has more than split_min
+// tail positions, so at most nnz / (split_min + 1) + 1 entries, and at most
+// nnz / 256 + entries chunks.
+struct SplitLayout {
+  int64_t entries, chunks;
+  size_t done, table, head, partial, total;
+};
+SplitLayout split_layout(int64_t nnz, int64_t split_min) {
+  auto up = [](size_t v) { return (v + 255) / 256 * 256; };
+  SplitLayout l;
+  l.entries = nnz / (split_min + 1) + 1;
+  l.chunks = nnz / kItems + l.entries + 1;
+  l.done = 256;
+  l.table = up(l.done + static_cast<size_t>(l.entries) * sizeof(int));
+  l.head = up(l.table + static_cast<size_t>(l.entries) * sizeof(SplitEntry));
+  l.partial = up(l.head + static_cast<size_t>(l.entries) * 8);
+  l.total = up(l.partial + static_cast<size_t>(l.chunks) * 8);
+  return l;
+}
+
+template <typename T>
+int split_typed(cudaStream_t s, int form, const ascb_csr* a, double alpha, double beta,
+                const ascb_vec* x, const ascb_vec* y, const int64_t* tiles, int64_t n, int sm,
+                const SplitBlock& b) {
+  const bool unit = x->stride == 1 && y->stride == 1;
+  const T al = static_cast<T>(alpha), be = static_cast<T>(beta);
+  if (form == ASCB_STANDARD) {
+    return unit ? launch_split<T, true, true>(s, a, al, be, x, y, tiles, n, sm, b)
+                : launch_split<T, true, false>(s, a, al, be, x, y, tiles, n, sm, b);
+  }
+  return unit ? launch_split<T, false, true>(s, a, al, be, x, y, tiles, n, sm, b)
+              : launch_split<T, false, false>(s, a, al, be, x, y, tiles, n, sm, b);
+}
+
+}  // namespace
+}  // namespace ascb
+
+extern "C" size_t ascb_split_bytes(int64_t nnz, int64_t split_min) {
+  if (split_min < ascb::kItems) split_min = ascb::kItems;
+  return ascb::split_layout(nnz, split_min).total;
+}
+
+extern "C" int ascb_spmv_split(void* stream, int dtype, int form, const ascb_csr* a, double alpha,
+                               double beta, const ascb_vec* x, const ascb_vec* y,
+                               const int64_t* tile_row, int64_t ntiles, int64_t split_min,
+                               void* block, int sm_count) {
+  if (ntiles <= 0) return 0;
+  if (split_min < ascb::kItems) split_min = ascb::kItems;
+  const ascb::SplitLayout l = ascb::split_layout(a->nnz, split_min);
+  auto* base = static_cast<unsigned char*>(block);
+  auto s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(block, 0, l.table, s);  // reservation word + finish counts
+  if (e != cudaSuccess) return static_cast<int>(e);
+  ascb::SplitBlock b;
+  b.packed = reinterpret_cast<unsigned long long*>(base);
+  b.done = reinterpret_cast<int*>(base + l.done);
+  b.entries = reinterpret_cast<ascb::SplitEntry*>(base + l.table);
+  b.head = base + l.head;
+  b.partial = base + l.partial;
+  b.max_entries = l.entries;
+  b.max_chunks = l.chunks;
+  b.split_min = split_min;
+  if (dtype == ASCB_F64) {
+    return ascb::split_typed<double>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count, b);
+  }
+  return ascb::split_typed<float>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count, b);
+}
 
 namespace ascb {
 namespace {

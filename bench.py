@@ -210,6 +210,43 @@ def run_reference(args, rank, world):
     return 0
 
 
+def headline_error(a, x, y_best, y_det, mode):
+    """Error of the headline product against the FP64 oracle (the C
+    restatement of SpmvReference; long double for the bound), and whether
+    the DETERMINISTIC product equals the oracle bit for bit."""
+    import oracle as orc
+    rs = orc.Restatement()
+    want = orc.compat_spmv_rows(rs, a.ptr, a.idx, a.val, 1.0, x, 0.0, np.zeros(a.rows))
+    exact, absval = orc.extended_rows(rs, a.cols, a.ptr, a.idx, a.val, x)
+    rep = orc.error_report(y_best, exact, absval, np.diff(a.ptr), np.float64, 1.0)
+    rep.update({"mode": mode, "bitexact": bool(y_best.tobytes() == want.tobytes()),
+                "deterministic_bitexact": bool(y_det.tobytes() == want.tobytes()),
+                "bound": "|y - y_ref| <= gamma_{n+2} |alpha| sum|a x| per row",
+                "oracle": "C restatement of SpmvReference (FP64), long double for the bound"})
+    return rep
+
+
+def cusparse_leg(a, A, x, stream, bytes_step):
+    """cuSPARSE SpMV (torch's CSR mat-vec) on the same device arrays: a
+    library comparison, timed like the headline; never the product."""
+    import torch
+    try:
+        with torch.cuda.stream(stream):
+            t = torch.sparse_csr_tensor(A.offsets, A.indices, A.values, (a.rows, a.cols))
+            torch.mv(t, x)
+        stream.synchronize()
+
+        def run():
+            with torch.cuda.stream(stream):
+                torch.mv(t, x)
+        ms = _timer(stream, 20, 3)(run)
+    except (RuntimeError, TypeError) as e:  # library refused the operands
+        return {"cusparse_csr_mv_unavailable": str(e)[:120]}
+    return {"cusparse_csr_mv_gbs": round(bytes_step / (ms * 1e-3) / 1e9, 2),
+            "cusparse_csr_mv_ms": round(ms, 4),
+            "note": "library comparison on the same arrays (torch CSR mat-vec), not the product"}
+
+
 def cpu_baseline_sample(a, x):
     """The reference's serial CPU SpMV (1 core) on a bounded row sample."""
     from oracle import Reference, Restatement, build_oracle
@@ -292,7 +329,8 @@ def run_gpu(args, rank, world):
                "warp_tiles": (Determinism.kBackendDefault, Variant.kWarpTiles, 0),
                "merge_path": (Determinism.kBackendDefault, Variant.kMergePath, 0),
                "vector_8": (Determinism.kBackendDefault, Variant.kVector, 8),
-               "vector_16": (Determinism.kBackendDefault, Variant.kVector, 16)}
+               "vector_16": (Determinism.kBackendDefault, Variant.kVector, 16),
+               "row_split": (Determinism.kBackendDefault, Variant.kRowSplit, 0)}
     if args.probe:
         # profiling aid: a few launches of one variant, nothing timed
         det, var, lanes = choices[args.probe]
@@ -385,8 +423,25 @@ def run_gpu(args, rank, world):
     last = (e2e_steps - 1) & 1
     e2e_ok = bool(torch.equal(y_pins[last], ys[last].cpu()))
 
-    # correctness of the last result against the oracle (rows sample)
+    # the headline's own result against the FP64 oracle (the checker; it runs
+    # after every timed region): the best mode's last product, and a
+    # DETERMINISTIC product compared bit for bit
     stream.synchronize()
+    error = None
+    if rank == 0:
+        ctx.set_determinism(Determinism.kDeterministic)
+        ctx.set_variant(Variant.kAuto, 0)
+        y_det = torch.zeros_like(y)
+        plan.csr_spmv(1.0, xv, 0.0, CudaStridedVectorView(y_det, a_h.rows))
+        stream.synchronize()
+        ctx.set_determinism(det)
+        ctx.set_variant(var, lanes)
+        plan.csr_spmv(1.0, xv, 0.0, yv)
+        stream.synchronize()
+        error = headline_error(a_h, x_h, y.cpu().numpy(), y_det.cpu().numpy(), best)
+    # comparison only (never the product): cuSPARSE through torch's CSR
+    # mat-vec on the same arrays, int64 indices
+    comparison = cusparse_leg(a_h, A, x, stream, bytes_step) if rank == 0 else None
     peak, peak_kind = _peaks()
     traffic = _traffic_record().get(WORKLOAD)
     out = None
@@ -419,6 +474,8 @@ def run_gpu(args, rank, world):
             "gpu_launches": int(launches * args.steps),
             "clocks": clk.summary(),
             "detail_gbs": {k: round(v, 2) for k, v in detail.items()},
+            "error_vs_fp64_oracle": error,
+            "comparison": comparison,
         }
     plan.close()
     ctx.close()
@@ -724,6 +781,73 @@ def run_extra(args):
     return 0
 
 
+def run_gather_floor(args):
+    """The floor under any CSR SpMV of the 4M-row power-law matrix: flat
+    (row-less) sums over its own column indices and values with one random
+    gather of x per nonzero, the gathers alone and the streamed arrays alone,
+    for each load pattern, gather flavour and CTAs per SM
+    (csrc/probe/gather_floor.cu).  One JSON line; `value` is the best flat
+    sum expressed in the SpMV byte model."""
+    import ctypes
+    import torch
+    from asc_cpp_b200 import build as lib_build
+
+    lib = ctypes.CDLL(lib_build.build_probe())
+    lib.ascb_probe_flat.restype = ctypes.c_int
+    lib.ascb_probe_flat.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64,
+                                    ctypes.c_int64, ctypes.c_void_p, ctypes.c_int]
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    a_h, x_h = _matrix()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    with torch.cuda.stream(stream):
+        idx = torch.from_numpy(a_h.idx).to(dev)
+        val = torch.from_numpy(a_h.val).to(dev)
+        x = torch.from_numpy(x_h).to(dev)
+        out = torch.zeros(sms * 16 * lib.ascb_probe_threads(), dtype=torch.float64, device=dev)
+    stream.synchronize()
+    nnz = a_h.nnz // 256 * 256
+    bytes_step = a_h.bytes_spmv(8)
+    timed = _timer(stream, max(5, min(args.steps, 50)), args.warmup)
+    names = {0: "flat_16B_lane_runs", 1: "flat_32B_lane_runs", 2: "flat_16B_coalesced",
+             3: "gathers_only", 4: "streams_only"}
+    flavours = {0: "nc", 1: "nc_L1_no_allocate", 2: "cg"}
+    table = {}
+    for mode, name in names.items():
+        for g, gname in flavours.items():
+            if mode == 4 and g > 0:
+                continue
+            for per_sm in (4, 6, 8, 12, 16):
+                def run():
+                    rc = lib.ascb_probe_flat(stream.cuda_stream, mode, g, idx.data_ptr(),
+                                             val.data_ptr(), x.data_ptr(), nnz, a_h.cols,
+                                             out.data_ptr(), sms * per_sm)
+                    if rc != 0:
+                        raise RuntimeError(f"probe launch failed: {rc}")
+                ms = timed(run)
+                table[f"{name}/{gname}/{per_sm}"] = round(ms, 4)
+    best = {name: min((v, k) for k, v in table.items() if k.startswith(name + "/"))
+            for name in names.values()}
+    flat = min(best[n] for n in ("flat_16B_lane_runs", "flat_32B_lane_runs", "flat_16B_coalesced"))
+    ms = flat[0]
+    gbs = bytes_step / (ms * 1e-3) / 1e9
+    peak, peak_kind = _peaks()
+    line = {"metric": "CSR SpMV gather floor (flat sum, SpMV byte model)", "value": round(gbs, 2),
+            "unit": "GB/s", "n_gpus": 1, "steps": max(5, min(args.steps, 50)),
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "gather_floor", "rows": a_h.rows, "nnz": a_h.nnz,
+                       "positions_timed": nnz, "bytes_per_step": bytes_step,
+                       "best": flat[1]},
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 2), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "traffic": None, "peak_kind": peak_kind},
+            "gathers_per_s_G": round(nnz / (best["gathers_only"][0] * 1e-3) / 1e9, 2),
+            "best_ms": {k: v for k, v in best.items()}, "table_ms": table}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
@@ -732,7 +856,8 @@ def main():
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--probe", default=None,
                    help="profiling aid: run 3 launches of one variant and exit")
-    p.add_argument("--workload", default=WORKLOAD, choices=(WORKLOAD,) + EXTRA,
+    p.add_argument("--workload", default=WORKLOAD,
+                   choices=(WORKLOAD,) + EXTRA + ("gather_floor",),
                    help="another configuration's workload (one GPU, this library only)")
     args = p.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -740,6 +865,8 @@ def main():
     world = _env_int("WORLD_SIZE", 1)
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "gather_floor":
+        return run_gather_floor(args)
     if args.workload != WORKLOAD:
         return run_extra(args)
     import torch.distributed as dist

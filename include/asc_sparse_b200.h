@@ -567,6 +567,75 @@ ASC_SB_API int asc_sb_batch_autotune(asc_sb_context* context,
                                      double beta, int32_t reps,
                                      float* best_ms);
 
+/* ---- storage sizes for clones into caller-owned memory --------------------- */
+
+/* Byte sizes of the three arrays of a CSR/CSC descriptor after the reference's
+ * metadata validation (ValidateSparseMetadata, operations.cc:134-251), so that
+ * a binding can allocate a clone's destination from the caller's memory
+ * resource -- as CloneCsrErased does (operations.cc:696-731) -- before
+ * asc_sb_clone_csr.  Nothing is touched on the device. */
+ASC_SB_API int asc_sb_sparse_storage_bytes(asc_sb_context* context,
+                                           const asc_sb_sparse* source,
+                                           size_t* offsets, size_t* indices,
+                                           size_t* values);
+/* The same for an indexed vector (ValidateIndexedMetadata,
+ * operations.cc:542-570), ahead of asc_sb_clone_indexed
+ * (CloneIndexedErased, operations.cc:802-830). */
+ASC_SB_API int asc_sb_indexed_storage_bytes(asc_sb_context* context,
+                                            const asc_sb_indexed_vector* source,
+                                            size_t* indices, size_t* values);
+
+/* ---- pointwise evaluation over one sparsity structure --------------------- */
+
+/* internal_sparse_cuda::PointwiseOperation and OperandKind (cuda.h:130-141). */
+enum {
+  ASC_SB_POINTWISE_COPY = 0,
+  ASC_SB_POINTWISE_NEGATE = 1,
+  ASC_SB_POINTWISE_ADD = 2,
+  ASC_SB_POINTWISE_SUBTRACT = 3,
+  ASC_SB_POINTWISE_MULTIPLY = 4
+};
+enum { ASC_SB_OPERAND_VIEW = 0, ASC_SB_OPERAND_SCALAR = 1 };
+
+/* internal_sparse_cuda::SparseDescriptor in full (cuda.h:143-156): any rank,
+ * for coordinate (ASC_SB_COORDINATE: structure_first holds nonzeros x rank
+ * int64 coordinates), CSR and CSC (rank two) storage. */
+typedef struct asc_sb_tensor {
+  const void* structure_first;
+  const void* structure_second;
+  const void* values;
+  int32_t memory_space;
+  int32_t element_kind;
+  int32_t format;
+  int32_t canonical_structure_trusted;
+  int64_t rank;
+  const int64_t* extents;  /* rank entries (host memory) */
+  int64_t nonzeros;
+} asc_sb_tensor;
+
+/* internal_sparse_cuda::OperandDescriptor (cuda.h:158-162): a view with the
+ * destination's structure, or a scalar whose element kind is view.element_kind. */
+typedef struct asc_sb_operand {
+  int32_t kind;
+  int32_t reserved;
+  asc_sb_tensor view;
+  double scalar;
+} asc_sb_operand;
+
+/* Replaces internal_sparse_cuda::EvaluateErased (cuda.h:228-231;
+ * operations.cc:1051-1120, kernel kernels.cu:118-158): for every stored
+ * position p, destination.values[p] = left[p] (copy), -left[p] (negate), or
+ * left[p] op right[p] (add, subtract, multiply), where a view operand reads
+ * its values at p and a scalar operand is its value converted to the element
+ * type.  View operands must share the destination's structure arrays (same
+ * pointers, format, rank, extents, nonzeros); a view's values may be the
+ * destination's values but may not partially overlap them.  float and
+ * double only, as the reference's public template allows. */
+ASC_SB_API int asc_sb_evaluate(asc_sb_context* context, int32_t operation,
+                               const asc_sb_operand* left,
+                               const asc_sb_operand* right,
+                               const asc_sb_tensor* destination);
+
 #ifdef __cplusplus
 }  /* extern "C" */
 #endif

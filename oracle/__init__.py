@@ -457,3 +457,118 @@ class Reference:
             op, triangle, diagonal, n, _ptr(ptr), _ptr(idx), _ptr(val), int(ptr[n]),
             rs(a.real), rs(a.imag), _ptr(b), layout, ld, k, b.size)
         return rc, b
+
+
+# ---- row-parallel drivers (full-size checks) --------------------------------
+#
+# For op = none every output row depends on that row's stored entries only,
+# and the restatement walks each row in stored order, so running disjoint row
+# blocks on separate threads gives the same bits as one serial call (ctypes
+# releases the GIL for the duration of each call).
+
+def _threads(threads: int | None) -> int:
+    if threads:
+        return threads
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return max(1, min(32, n))
+
+
+def row_blocks(ptr: np.ndarray, parts: int) -> list[tuple[int, int]]:
+    """Up to ``parts`` contiguous row blocks with about equal stored entries
+    plus rows each."""
+    rows = len(ptr) - 1
+    if rows <= 0:
+        return []
+    weight_total = int(ptr[-1]) + rows
+    cuts = [0]
+    for k in range(1, parts):
+        target = weight_total * k // parts
+        # first row r with ptr[r] + r >= target
+        lo, hi = cuts[-1], rows
+        while lo < hi:
+            mid = (lo + hi) // 2
+            if int(ptr[mid]) + mid < target:
+                lo = mid + 1
+            else:
+                hi = mid
+        if lo > cuts[-1]:
+            cuts.append(lo)
+    cuts.append(rows)
+    return [(a, b) for a, b in zip(cuts[:-1], cuts[1:]) if b > a]
+
+
+def _run_blocks(fn, ptr, threads):
+    from concurrent.futures import ThreadPoolExecutor
+    blocks = row_blocks(ptr, 4 * _threads(threads))
+    with ThreadPoolExecutor(max_workers=_threads(threads)) as ex:
+        for f in [ex.submit(fn, r0, r1) for r0, r1 in blocks]:
+            f.result()
+
+
+def compat_spmv_rows(rs: "Restatement", ptr, idx, val, alpha, x, beta, y, threads=None):
+    """Restatement.compat_spmv (unit strides) over row blocks in parallel."""
+    _run_blocks(lambda r0, r1: rs.compat_spmv(ptr[r0:r1 + 1], idx, val, alpha, x, beta,
+                                              y[r0:r1]), ptr, threads)
+    return y
+
+
+def standard_spmv_rows(rs: "Restatement", cols, ptr, idx, val, alpha, x, y, threads=None):
+    """y += alpha*A*x (CSR, op none, unit strides) over row blocks in parallel."""
+    _run_blocks(lambda r0, r1: rs.standard_spmv(CSR, OP_NONE, r1 - r0, cols, ptr[r0:r1 + 1],
+                                                idx, val, alpha, x, y[r0:r1]), ptr, threads)
+    return y
+
+
+def standard_spmm_rows(rs: "Restatement", cols, ptr, idx, val, alpha, b, c, threads=None):
+    """C += alpha*A*B (CSR, op none, row-major B [cols, k] and C [rows, k],
+    contiguous) over row blocks in parallel."""
+    k = b.shape[1]
+    _run_blocks(lambda r0, r1: rs.standard_spmm(CSR, OP_NONE, r1 - r0, cols, ptr[r0:r1 + 1],
+                                                idx, val, alpha, b, ROW_MAJOR, k, c[r0:r1],
+                                                ROW_MAJOR, k, k), ptr, threads)
+    return c
+
+
+def extended_rows(rs: "Restatement", cols, ptr, idx, val, x, threads=None):
+    """Restatement.extended for op none over row blocks in parallel: the
+    long-double sum and sum of |products| of every row."""
+    rows = len(ptr) - 1
+    exact = np.zeros(rows, dtype=np.longdouble)
+    absval = np.zeros(rows, dtype=np.longdouble)
+
+    def part(r0, r1):
+        e, a = rs.extended(OP_NONE, r1 - r0, cols, ptr[r0:r1 + 1], idx, val, x)
+        exact[r0:r1] = e
+        absval[r0:r1] = a
+    _run_blocks(part, ptr, threads)
+    return exact, absval
+
+
+def gamma(n, dtype) -> np.ndarray:
+    """gamma_n = n u / (1 - n u), u the unit roundoff of ``dtype``."""
+    u = np.finfo(dtype).eps / 2
+    n = np.asarray(n, np.float64)
+    return n * u / (1 - n * u)
+
+
+def error_report(got, reference, absval, counts, dtype, alpha, beta_abs=0.0,
+                 reference_abs_err=0.0) -> dict:
+    """Error of ``got`` against ``reference`` (an FP64 or long-double oracle
+    value), and the largest ratio to the stated bound
+        |y - y_ref| <= gamma_{n+2}(|alpha| sum|a x| + |beta y0|) + tiny
+    (plus ``reference_abs_err``, the reference's own error bound, when the
+    reference is not exact).  ``max_ratio_to_bound`` <= 1 means within."""
+    got = np.asarray(got, np.float64)
+    ref = np.asarray(reference, np.float64)
+    bound = gamma(np.asarray(counts) + 2, dtype) * (
+        abs(alpha) * np.asarray(absval, np.float64) + beta_abs)
+    bound = bound + reference_abs_err + np.finfo(dtype).tiny
+    err = np.abs(got - ref)
+    scale = np.maximum(np.abs(ref), np.finfo(np.float64).tiny)
+    return {"max_abs": float(err.max()) if err.size else 0.0,
+            "max_rel": float((err / scale).max()) if err.size else 0.0,
+            "max_ratio_to_bound": float((err / bound).max()) if err.size else 0.0,
+            "outputs": int(err.size)}

@@ -62,10 +62,13 @@ def test_descriptor_layouts_match_header():
 #include <stdio.h>
 #include "asc_sparse_b200.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(asc_sb_sparse), sizeof(asc_sb_vector),
-         sizeof(asc_sb_dense), offsetof(asc_sb_sparse, rows), offsetof(asc_sb_vector, extent),
-         offsetof(asc_sb_dense, leading_dimension), offsetof(asc_sb_dense, writable),
-         sizeof(asc_sb_indexed_vector), offsetof(asc_sb_indexed_vector, dense_extent));
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu %zu\n", sizeof(asc_sb_sparse),
+         sizeof(asc_sb_vector), sizeof(asc_sb_dense), offsetof(asc_sb_sparse, rows),
+         offsetof(asc_sb_vector, extent), offsetof(asc_sb_dense, leading_dimension),
+         offsetof(asc_sb_dense, writable), sizeof(asc_sb_indexed_vector),
+         offsetof(asc_sb_indexed_vector, dense_extent), sizeof(asc_sb_tensor),
+         offsetof(asc_sb_tensor, extents), sizeof(asc_sb_operand),
+         offsetof(asc_sb_operand, scalar));
   return 0;
 }
 '''
@@ -81,7 +84,9 @@ int main(void) {
             ctypes.sizeof(_abi.DenseDesc), _abi.SparseDesc.rows.offset,
             _abi.VectorDesc.extent.offset, _abi.DenseDesc.leading_dimension.offset,
             _abi.DenseDesc.writable.offset, ctypes.sizeof(_abi.IndexedDesc),
-            _abi.IndexedDesc.dense_extent.offset]
+            _abi.IndexedDesc.dense_extent.offset, ctypes.sizeof(_abi.TensorDesc),
+            _abi.TensorDesc.extents.offset, ctypes.sizeof(_abi.OperandDesc),
+            _abi.OperandDesc.scalar.offset]
     assert got == want
 
 
