@@ -81,8 +81,10 @@ class Variant(IntEnum):
 
 PLAN_TRANSPOSE = 1
 PLAN_TRIANGULAR = 2
+PLAN_ROW_GROUPS = 4
 PLAN_HAS_TRANSPOSE = 1
 PLAN_HAS_BLOCKS16 = 2
+PLAN_HAS_ROW_GROUPS = 4
 
 
 class SparseDesc(ctypes.Structure):
@@ -191,6 +193,8 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_context_destroy": (ctypes.c_int, [_P]),
     "asc_sb_context_set_determinism": (ctypes.c_int, [_P, _I32]),
     "asc_sb_context_set_variant": (ctypes.c_int, [_P, _I32, _I32]),
+    "asc_sb_context_set_wait_limit": (ctypes.c_int, [_P, _I64]),
+    "asc_sb_context_set_allocator": (ctypes.c_int, [_P, _P, _P, _P]),
     "asc_sb_context_stream": (_P, [_P]),
     "asc_sb_context_synchronize": (ctypes.c_int, [_P]),
     "asc_sb_context_last_error": (ctypes.c_char_p, [_P]),
@@ -208,6 +212,9 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_csr_spmv": (ctypes.c_int, [_P, _P, _D, _VP, _D, _VP]),
     "asc_sb_plan_standard_spmv": (ctypes.c_int, [_P, _P, _I32, _D, _D, _VP, _VP]),
     "asc_sb_plan_standard_spmm": (ctypes.c_int, [_P, _P, _I32, _D, _D, _DP, _DP]),
+    "asc_sb_plan_spmm_autotune": (ctypes.c_int, [_P, _P, _D, _DP, _DP, _I32,
+                                                 ctypes.POINTER(ctypes.c_float),
+                                                 ctypes.POINTER(_I32)]),
     "asc_sb_standard_triangular_solve": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _I32, _I32,
                                                         _DP]),
     "asc_sb_plan_triangular_solve": (ctypes.c_int, [_P, _P, _I32, _D, _D, _I32, _I32, _DP]),

@@ -39,6 +39,7 @@ def _headers() -> list[str]:
     return (glob.glob(os.path.join(CSRC, "*.h")) +
             glob.glob(os.path.join(CSRC, "*.cuh")) +
             glob.glob(os.path.join(CSRC, "host", "*.h")) +
+            glob.glob(os.path.join(CSRC, "host", "*.inc")) +
             glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 

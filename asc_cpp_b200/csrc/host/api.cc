@@ -18,6 +18,7 @@
 #include "../../../include/asc_sparse_b200.h"
 #include "../kernels.h"
 #include "context_view.h"
+#include "memory.h"
 #include "validate.h"
 
 using ascb::host::Fail;
@@ -37,6 +38,7 @@ struct asc_sb_context {
   std::string last_error;
   std::atomic<std::int64_t> launches{0};
   int* status = nullptr;  // device word: kernels record bounded-wait timeouts
+  std::uint64_t wait_ns = 0;  // dependency-wait limit of solves (0: the kernels' 2 s)
   void* scratch = nullptr;  // kContextScratch device bytes after the status word
   // installed variant selector: device parameters and scratch, and the
   // variant (id, lanes) each MLP output stands for
@@ -46,8 +48,30 @@ struct asc_sb_context {
   // triangular solves without a plan: ready flags (and, for transposed
   // solves, the transposed structure) in a buffer that grows to the largest
   // solve seen
-  void* solve_scratch = nullptr;
-  std::size_t solve_bytes = 0;
+  ascb::host::Block solve_mem;
+  ascb::host::Block selector_mem;  // holds `selector`
+  ascb::host::Allocator allocator;  // for the blocks above and clone staging
+  // selector picks of matrices used without a plan (ChooseWithoutPlan)
+  struct PickKey {
+    const void* ptr = nullptr;
+    const void* idx = nullptr;
+    const void* val = nullptr;
+    std::int64_t rows = 0, cols = 0, nnz = 0;
+    std::int32_t kind = 0, format = 0;
+    bool operator==(const PickKey&) const = default;
+  };
+  struct PickSlot {
+    PickKey key;
+    int state = 0;  // 0 empty, 1 selection in flight, 2 pick ready
+    int pick = -1;
+    std::uint64_t used = 0;
+    cudaEvent_t done = nullptr;
+  };
+  static constexpr int kPickSlots = 16;
+  PickSlot picks[kPickSlots];
+  ascb::host::Block pick_words;  // pinned host: one int per slot
+  int pick_in_flight = -1;
+  std::uint64_t pick_clock = 0;
   void* stager = nullptr;  // clone staging, clone.cc
 };
 
@@ -89,9 +113,16 @@ struct asc_sb_plan {
   bool analysis_lower = false;       // of a lower triangular op(A)
   const std::int64_t* order = nullptr;
   const std::int64_t* position = nullptr;
+  // ASC_SB_PLAN_ROW_GROUPS: runs of R consecutive rows for the row-group SpMM
+  unsigned char* groups_mem = nullptr;
+  ascb_row_groups groups{};
+  std::int64_t group_run_count = 0;
+  bool use_groups = false;  // SpMM through the groups (reuse measured or tuned)
 };
 
 namespace {
+
+#include "selector_default.inc"
 
 constexpr std::size_t kWorkspaceAlignment = 16;  // alignof(std::max_align_t)
 
@@ -355,7 +386,7 @@ std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
 struct PlanLayout {
   std::size_t flag = 0;  // one device int for structure checks
   std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, t_part = 0;
-  std::size_t sort = 0, outer_of = 0, solve = 0, analysis = 0, total = 0;
+  std::size_t sort = 0, outer_of = 0, solve = 0, analysis = 0, groups = 0, total = 0;
 };
 
 PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
@@ -391,8 +422,42 @@ PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
     l.analysis = at;
     at += RoundUp(ascb_trsv_analysis_bytes(outer), 256);
   }
+  if (flags & ASC_SB_PLAN_ROW_GROUPS) {
+    l.groups = at;
+    at += RoundUp(ascb_row_groups_layout_for(
+                      outer, nnz, static_cast<int>(ascb::host::ElementBytes(m.element_kind)))
+                      .total,
+                  256);
+  }
   l.total = at;
   return l;
+}
+
+// Row groups of R rows for the plan's CSR arrays; reads back the number of
+// runs (synchronizes the stream) and keeps the groups in use when they share
+// B rows: at least 1.25 stored entries per run.
+constexpr int kDefaultRowsPerGroup = 8;
+Status BuildRowGroups(asc_sb_context* ctx, asc_sb_plan* plan, int rows_per_group) {
+  const ascb_csr a = AsCsr(plan->matrix, false);
+  const int elem = static_cast<int>(ascb::host::ElementBytes(plan->matrix.element_kind));
+  Status s = Launched(ctx,
+                      ascb_row_groups_build(ctx->stream, &a, elem, rows_per_group,
+                                            plan->groups_mem, &plan->groups, ctx->sm_count),
+                      "CUDA could not launch the row-group build");
+  if (!s.ok()) return s;
+  const std::int64_t groups = (a.rows + rows_per_group - 1) / rows_per_group;
+  std::int64_t runs = 0;
+  cudaError_t e = cudaMemcpyAsync(&runs, plan->groups.group_runs + groups, sizeof(runs),
+                                  cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return {ASC_SB_PROVIDER, std::string("CUDA could not build the row groups: ") +
+                                 cudaGetErrorString(e)};
+  }
+  plan->group_run_count = runs;
+  plan->use_groups = runs > 0 && 4 * a.nnz >= 5 * runs;
+  return Status::Ok();
 }
 
 // Stable transposed structure of the CSR arrays `a` (rows = stored outer
@@ -453,6 +518,116 @@ Status SelectVariant(asc_sb_context* ctx, asc_sb_plan* plan) {
   plan->variant = ctx->selector_variant[static_cast<std::size_t>(pick)];
   plan->lanes = ctx->selector_lanes[static_cast<std::size_t>(pick)];
   return Status::Ok();
+}
+
+// Variant of a real, non-transposed product without a plan.  With a selector
+// installed (BACKEND_DEFAULT, variant AUTO) the first call on a matrix --
+// keyed by its arrays and shape -- enqueues the selection (features -> MLP ->
+// argmin -> a pinned host word, then an event) ahead of its own product, which
+// runs the default; later calls use the pick once the event has completed.  No
+// host wait, and nothing is enqueued while the stream is being captured.  A
+// stale key (arrays freed and reused for another matrix of the same shape)
+// only costs speed: every variant meets the same bound.
+Choice ChooseWithoutPlan(asc_sb_context* ctx, const asc_sb_sparse& m) {
+  Choice c = Choose(ctx, m);
+  if (ctx->determinism == ASC_SB_DETERMINISTIC || ctx->variant != ASC_SB_VARIANT_AUTO ||
+      ctx->selector == nullptr || !RealKind(m.element_kind) || m.nonzeros == 0) {
+    return c;
+  }
+  auto& slots = ctx->picks;
+  const int* words = static_cast<const int*>(ctx->pick_words.ptr);
+  if (ctx->pick_in_flight >= 0) {  // has the selection in flight landed?
+    auto& f = slots[ctx->pick_in_flight];
+    const cudaError_t q = cudaEventQuery(f.done);
+    if (q == cudaSuccess) {
+      const int pick = words[ctx->pick_in_flight];
+      f.state = pick >= 0 && pick < ctx->selector_outputs ? 2 : 0;
+      f.pick = pick;
+      ctx->pick_in_flight = -1;
+    } else if (q != cudaErrorNotReady) {
+      (void)cudaGetLastError();
+      f.state = 0;
+      ctx->pick_in_flight = -1;
+    }
+  }
+  asc_sb_context::PickKey key{m.structure_first, m.structure_second, m.values, m.rows,
+                              m.columns, m.nonzeros, m.element_kind, m.format};
+  int victim = -1;
+  for (int i = 0; i < asc_sb_context::kPickSlots; ++i) {
+    auto& slot = slots[i];
+    if (slot.state != 0 && slot.key == key) {
+      slot.used = ++ctx->pick_clock;
+      if (slot.state == 2) {
+        c.variant = ctx->selector_variant[static_cast<std::size_t>(slot.pick)];
+        const int lanes = ctx->selector_lanes[static_cast<std::size_t>(slot.pick)];
+        c.lanes = lanes > 0 ? lanes : AutoLanes(m, false);
+      }
+      return c;
+    }
+    if (slot.state != 1 && (victim < 0 || slot.state == 0 ||
+                            (slots[victim].state != 0 && slot.used < slots[victim].used))) {
+      victim = i;
+    }
+  }
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  if (ctx->pick_in_flight >= 0 || victim < 0 ||
+      cudaStreamIsCapturing(ctx->stream, &capture) != cudaSuccess ||
+      capture != cudaStreamCaptureStatusNone) {
+    (void)cudaGetLastError();
+    return c;
+  }
+  if (ctx->pick_words.ptr == nullptr &&
+      !ascb::host::Acquire(ctx->allocator, sizeof(int) * asc_sb_context::kPickSlots,
+                           ASC_SB_PINNED_HOST, &ctx->pick_words)) {
+    return c;  // no room for the answers: keep the default
+  }
+  auto& slot = slots[victim];
+  if (slot.done == nullptr &&
+      cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming) != cudaSuccess) {
+    (void)cudaGetLastError();
+    slot.done = nullptr;
+    return c;
+  }
+  float* base = ctx->selector;
+  const ascb_csr a = AsCsr(m, m.format == ASC_SB_CSC);
+  int* word = static_cast<int*>(ctx->pick_words.ptr) + victim;
+  int rc = ascb_matrix_features(
+      ctx->stream, &a, static_cast<int>(ascb::host::ElementBytes(m.element_kind)),
+      reinterpret_cast<unsigned long long*>(base + kSelAcc), base + kSelFeatures, ctx->sm_count);
+  if (rc == 0) {
+    rc = ascb_mlp_forward(ctx->stream, ctx->selector_outputs, base + kSelParams,
+                          base + kSelFeatures, 1, base + kSelHidden, base + kSelOut);
+  }
+  if (rc == 0) {
+    rc = ascb_argmin(ctx->stream, base + kSelOut, ctx->selector_outputs,
+                     reinterpret_cast<int*>(base + kSelPick));
+  }
+  ctx->launches.fetch_add(6, std::memory_order_relaxed);
+  if (rc == 0) {
+    rc = static_cast<int>(cudaMemcpyAsync(word, base + kSelPick, sizeof(int),
+                                          cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  if (rc == 0) rc = static_cast<int>(cudaEventRecord(slot.done, ctx->stream));
+  if (rc != 0) {
+    (void)cudaGetLastError();
+    slot.state = 0;
+    return c;
+  }
+  slot.key = key;
+  slot.state = 1;
+  slot.pick = -1;
+  slot.used = ++ctx->pick_clock;
+  ctx->pick_in_flight = victim;
+  return c;
+}
+
+// Forgets every pick (a new selector was installed); the stream is idle.
+void ForgetPicks(asc_sb_context* ctx) {
+  for (auto& slot : ctx->picks) {
+    slot.state = 0;
+    slot.pick = -1;
+  }
+  ctx->pick_in_flight = -1;
 }
 
 // Marks the plan when its matrix is made of dense 16 x 16 blocks (one check
@@ -565,6 +740,13 @@ int asc_sb_context_create(int32_t device, void* stream, asc_sb_context** out) {
     return ASC_SB_ALLOCATION;
   }
   ctx->scratch = reinterpret_cast<unsigned char*>(ctx->status) + kContextScratchOffset;
+  // the shipped selector: BACKEND_DEFAULT products with variant AUTO pick
+  // their kernel from the start; a context that cannot hold it still works
+  // and runs the default variant
+  if (asc_sb_context_set_selector(ctx, kDefaultSelectorOutputs, kDefaultSelectorParams,
+                                  kDefaultSelectorVariants, kDefaultSelectorLanes) != ASC_SB_OK) {
+    ctx->last_error.clear();
+  }
   *out = ctx;
   return ASC_SB_OK;
 }
@@ -575,8 +757,12 @@ int asc_sb_context_destroy(asc_sb_context* ctx) {
   (void)cudaStreamSynchronize(ctx->stream);
   if (ctx->owns_stream) (void)cudaStreamDestroy(ctx->stream);
   if (ctx->status != nullptr) (void)cudaFree(ctx->status);
-  if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
-  if (ctx->solve_scratch != nullptr) (void)cudaFree(ctx->solve_scratch);
+  for (auto& slot : ctx->picks) {
+    if (slot.done != nullptr) (void)cudaEventDestroy(slot.done);
+  }
+  ascb::host::Release(&ctx->pick_words);
+  ascb::host::Release(&ctx->selector_mem);
+  ascb::host::Release(&ctx->solve_mem);
   ascb::host::DestroyStager(ctx->stager);
   delete ctx;
   return ASC_SB_OK;
@@ -619,6 +805,25 @@ int asc_sb_context_set_variant(asc_sb_context* ctx, int32_t variant, int32_t lan
   std::lock_guard<std::mutex> lock(ctx->mutex);
   ctx->variant = variant;
   ctx->lanes = lanes;
+  return ASC_SB_OK;
+}
+
+int asc_sb_context_set_allocator(asc_sb_context* ctx, asc_sb_allocate_fn allocate,
+                                 asc_sb_deallocate_fn release, void* user) {
+  if (ctx == nullptr) return ASC_SB_INVALID_STATE;
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  ctx->allocator = allocate != nullptr ? ascb::host::Allocator{allocate, release, user}
+                                       : ascb::host::Allocator{};
+  return ASC_SB_OK;
+}
+
+int asc_sb_context_set_wait_limit(asc_sb_context* ctx, int64_t nanoseconds) {
+  if (ctx == nullptr) return ASC_SB_INVALID_STATE;
+  if (nanoseconds < 0) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "The wait limit cannot be negative"));
+  }
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  ctx->wait_ns = static_cast<std::uint64_t>(nanoseconds);
   return ASC_SB_OK;
 }
 
@@ -710,7 +915,7 @@ int asc_sb_csr_spmv(asc_sb_context* ctx, double alpha, const asc_sb_sparse* m,
   }
   const ascb_csr a = AsCsr(*m, false);
   const ascb_vec xv = AsVec(*x), yv = AsVec(*y);
-  const Choice choice = Choose(ctx, *m);
+  const Choice choice = ChooseWithoutPlan(ctx, *m);
   s = RunCsr(ctx, choice, ASCB_COMPAT, a, Dtype(m->element_kind), alpha, beta, xv, yv,
              tile_buffer, nullptr);
   return Finish(ctx, s);
@@ -795,7 +1000,7 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
   }
   if (!transposed) {
     const Choice choice = plan != nullptr ? Choose(ctx, m, plan->variant, plan->lanes)
-                                          : Choose(ctx, m);
+                                          : ChooseWithoutPlan(ctx, m);
     return RunCsr(ctx, choice, ASCB_STANDARD, a, dtype, alpha, 0.0, xv, yv, nullptr,
                   plan != nullptr ? &plan->part : nullptr);
   }
@@ -834,6 +1039,17 @@ int asc_sb_standard_spmv(asc_sb_context* ctx, int32_t op, double alpha_real, dou
 
 // ---------------------------------------------------------------------------
 namespace {
+
+// The row-group kernel's operand rules: row-major B and C whose rows are
+// whole 16-byte chunks on 16-byte boundaries.
+bool GroupsApply(const asc_sb_dense& b, const asc_sb_dense& c, int kind) {
+  const std::int64_t n = kind == ASC_SB_DOUBLE ? 2 : 4;
+  return (kind == ASC_SB_FLOAT || kind == ASC_SB_DOUBLE) && b.layout == ASC_SB_ROW_MAJOR &&
+         c.layout == ASC_SB_ROW_MAJOR && c.columns % n == 0 && b.leading_dimension % n == 0 &&
+         c.leading_dimension % n == 0 &&
+         ((reinterpret_cast<std::uintptr_t>(b.data) | reinterpret_cast<std::uintptr_t>(c.data)) &
+          15u) == 0;
+}
 
 // C += alpha * op(A) * B, validated in full before anything is enqueued.  With
 // a plan that holds the transposed structure, a transposed product runs the
@@ -904,6 +1120,16 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
                                       ctx->sm_count),
                     "CUDA could not launch the complex SpMM kernel");
   }
+  if (!transposed && !csc && plan != nullptr && plan->use_groups &&
+      GroupsApply(*b, *c, m->element_kind)) {
+    return Launched(ctx,
+                    ascb_spmm_groups(ctx->stream, Dtype(m->element_kind),
+                                     ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0, &a,
+                                     &plan->groups, c->columns, b->data, b->leading_dimension,
+                                     const_cast<void*>(c->data), c->leading_dimension,
+                                     alpha_real, ctx->sm_count),
+                    "CUDA could not launch the row-group SpMM kernel");
+  }
   return Launched(ctx,
                   ascb_spmm(ctx->stream, Dtype(m->element_kind), transposed && !planned ? 1 : 0,
                             ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0, &a, c->columns, b->data, b->layout, b->leading_dimension,
@@ -932,7 +1158,7 @@ int asc_sb_plan_workspace_size(asc_sb_context* ctx, const asc_sb_sparse* m, int3
   if (m == nullptr || bytes == nullptr) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "plan arguments cannot be null"));
   }
-  if ((flags & ~(ASC_SB_PLAN_TRANSPOSE | ASC_SB_PLAN_TRIANGULAR)) != 0) {
+  if ((flags & ~(ASC_SB_PLAN_TRANSPOSE | ASC_SB_PLAN_TRIANGULAR | ASC_SB_PLAN_ROW_GROUPS)) != 0) {
     return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "unknown plan flags"));
   }
   if (m->rows < 0 || m->columns < 0 || m->nonzeros < 0) {
@@ -991,6 +1217,12 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
       m->rows % 16 == 0 && m->nonzeros > 0 &&
       (reinterpret_cast<std::uintptr_t>(m->values) & 15u) == 0) {
     s = DetectBlocks(ctx, a, reinterpret_cast<int*>(ws + PlanLayoutFor(*m, flags).flag), plan);
+  }
+  // (run offsets are 32-bit: groups are built below 2^32 stored entries)
+  if (s.ok() && (flags & ASC_SB_PLAN_ROW_GROUPS) && m->format == ASC_SB_CSR &&
+      RealKind(m->element_kind) && m->rows > 0 && m->nonzeros < (std::int64_t{1} << 32)) {
+    plan->groups_mem = ws + PlanLayoutFor(*m, flags).groups;
+    s = BuildRowGroups(ctx, plan, kDefaultRowsPerGroup);
   }
   if (s.ok() && ctx->selector != nullptr && ctx->determinism != ASC_SB_DETERMINISTIC &&
       ctx->variant == ASC_SB_VARIANT_AUTO && RealKind(m->element_kind)) {
@@ -1383,24 +1615,19 @@ namespace {
 // Grows the context's solve buffer to `bytes`.  A larger buffer replaces the
 // old one only after the stream has finished with it.
 Status SolveScratch(asc_sb_context* ctx, std::size_t bytes, unsigned char** out) {
-  if (ctx->solve_bytes < bytes) {
-    if (ctx->solve_scratch != nullptr) {
+  if (ctx->solve_mem.bytes < bytes) {
+    if (ctx->solve_mem.ptr != nullptr) {
       if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
         (void)cudaGetLastError();
         return Fail(ASC_SB_PROVIDER, "CUDA could not drain the stream before growing scratch");
       }
-      (void)cudaFree(ctx->solve_scratch);
-      ctx->solve_scratch = nullptr;
-      ctx->solve_bytes = 0;
+      ascb::host::Release(&ctx->solve_mem);
     }
-    if (cudaMalloc(&ctx->solve_scratch, bytes) != cudaSuccess) {
-      (void)cudaGetLastError();
-      ctx->solve_scratch = nullptr;
-      return Fail(ASC_SB_ALLOCATION, "CUDA could not allocate triangular-solve scratch");
+    if (!ascb::host::Acquire(ctx->allocator, bytes, ASC_SB_DEVICE, &ctx->solve_mem)) {
+      return Fail(ASC_SB_ALLOCATION, "could not allocate triangular-solve scratch");
     }
-    ctx->solve_bytes = bytes;
   }
-  *out = static_cast<unsigned char*>(ctx->solve_scratch);
+  *out = static_cast<unsigned char*>(ctx->solve_mem.ptr);
   return Status::Ok();
 }
 
@@ -1510,6 +1737,7 @@ Status TriangularSolve(asc_sb_context* ctx, const asc_sb_plan* plan, int op, dou
     t.position = plan->position;
   }
   t.status = ctx->status;
+  t.wait_ns = ctx->wait_ns;
   return Launched(ctx,
                   ascb_sptrsv(ctx->stream, Dtype(m->element_kind),
                               ctx->determinism == ASC_SB_DETERMINISTIC, alpha_zero, &t,
@@ -1566,6 +1794,7 @@ int asc_sb_plan_triangular_analysis(asc_sb_context* ctx, asc_sb_plan* plan, int3
   t.lower = transposed ? triangle == ASC_SB_UPPER : triangle == ASC_SB_LOWER;
   t.control = plan->solve;
   t.status = ctx->status;
+  t.wait_ns = ctx->wait_ns;
   std::int64_t* order = nullptr;
   std::int64_t* position = nullptr;
   plan->analysed = false;
@@ -1610,9 +1839,10 @@ int asc_sb_context_set_selector(asc_sb_context* ctx, int32_t n_variants, const f
   if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
   if (params == nullptr) {  // remove
     (void)cudaStreamSynchronize(ctx->stream);
-    if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
+    ascb::host::Release(&ctx->selector_mem);
     ctx->selector = nullptr;
     ctx->selector_outputs = 0;
+    ForgetPicks(ctx);
     return Finish(ctx, Status::Ok());
   }
   if (n_variants < 1 || n_variants > kSelMaxOutputs || variants == nullptr || lanes == nullptr) {
@@ -1625,21 +1855,23 @@ int asc_sb_context_set_selector(asc_sb_context* ctx, int32_t n_variants, const f
   }
   const std::size_t count = static_cast<std::size_t>(ascb_mlp_param_count(n_variants));
   const std::size_t bytes = (kSelParams + count) * sizeof(float);
-  (void)cudaStreamSynchronize(ctx->stream);
-  if (ctx->selector != nullptr) (void)cudaFree(ctx->selector);
-  ctx->selector = nullptr;
-  float* dev = nullptr;
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&dev), bytes);
-  if (e == cudaSuccess) {
-    e = cudaMemcpy(dev + kSelParams, params, count * sizeof(float), cudaMemcpyHostToDevice);
+  ascb::host::Block mem;
+  if (!ascb::host::Acquire(ctx->allocator, bytes, ASC_SB_DEVICE, &mem)) {
+    return Finish(ctx, Fail(ASC_SB_ALLOCATION, "could not allocate the selector's parameters"));
   }
-  if (e != cudaSuccess) {
-    if (dev != nullptr) (void)cudaFree(dev);
+  float* dev = static_cast<float*>(mem.ptr);
+  const cudaError_t e = cudaMemcpyAsync(dev + kSelParams, params, count * sizeof(float),
+                                        cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess || cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
     (void)cudaGetLastError();
-    return Finish(ctx, {ASC_SB_ALLOCATION, std::string("could not install the selector: ") +
-                                               cudaGetErrorString(e)});
+    ascb::host::Release(&mem);
+    return Finish(ctx, Fail(ASC_SB_MEMORY_TRANSFER, "could not copy the selector's parameters"));
   }
+  // the new parameters replace the old ones only once they are in place
+  ascb::host::Release(&ctx->selector_mem);
+  ctx->selector_mem = mem;
   ctx->selector = dev;
+  ForgetPicks(ctx);
   ctx->selector_outputs = n_variants;
   ctx->selector_variant.assign(variants, variants + n_variants);
   ctx->selector_lanes.assign(lanes, lanes + n_variants);
@@ -1649,7 +1881,8 @@ int asc_sb_context_set_selector(asc_sb_context* ctx, int32_t n_variants, const f
 int asc_sb_plan_properties(const asc_sb_plan* plan, int32_t* properties) {
   if (plan == nullptr || properties == nullptr) return ASC_SB_INVALID_ARGUMENT;
   *properties = (plan->t_ptr != nullptr ? ASC_SB_PLAN_HAS_TRANSPOSE : 0) |
-                (plan->block16 ? ASC_SB_PLAN_HAS_BLOCKS16 : 0);
+                (plan->block16 ? ASC_SB_PLAN_HAS_BLOCKS16 : 0) |
+                (plan->use_groups ? ASC_SB_PLAN_HAS_ROW_GROUPS : 0);
   return ASC_SB_OK;
 }
 
@@ -1658,6 +1891,62 @@ int asc_sb_plan_variant(const asc_sb_plan* plan, int32_t* variant, int32_t* lane
   *variant = plan->variant >= -1 ? plan->variant : ASC_SB_VARIANT_AUTO;
   *lanes = plan->lanes;
   return ASC_SB_OK;
+}
+
+int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alpha,
+                              const asc_sb_dense* b, const asc_sb_dense* c, int32_t reps,
+                              float* best_ms, int32_t* rows_per_group) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr || b == nullptr || c == nullptr || reps < 1 || best_ms == nullptr ||
+      rows_per_group == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "SpMM autotune arguments are invalid"));
+  }
+  if (plan->groups_mem == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_STATE,
+                            "SpMM autotuning needs a plan created with ASC_SB_PLAN_ROW_GROUPS"));
+  }
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  // candidates: 0 = the row-by-row kernel, else R rows per group
+  const int candidates[] = {0, 2, 4, 8, 16, 32};
+  cudaEvent_t start = nullptr, stop = nullptr;
+  cudaError_t e = cudaEventCreate(&start);
+  if (e == cudaSuccess) e = cudaEventCreate(&stop);
+  int best = -1;
+  float best_time = 0.0f;
+  for (int rg : candidates) {
+    if (!s.ok() || e != cudaSuccess) break;
+    if (rg != 0 && plan->groups.rows_per_group != rg) s = BuildRowGroups(ctx, plan, rg);
+    if (!s.ok()) break;
+    plan->use_groups = rg != 0;
+    s = StandardSpmm(ctx, plan, ASC_SB_OP_NONE, alpha, 0.0, &plan->matrix, b, c);  // warm-up
+    if (s.ok()) e = cudaEventRecord(start, ctx->stream);
+    for (int r = 0; r < reps && s.ok() && e == cudaSuccess; ++r) {
+      s = StandardSpmm(ctx, plan, ASC_SB_OP_NONE, alpha, 0.0, &plan->matrix, b, c);
+    }
+    if (s.ok() && e == cudaSuccess) e = cudaEventRecord(stop, ctx->stream);
+    if (s.ok() && e == cudaSuccess) e = cudaEventSynchronize(stop);
+    float t = 0.0f;
+    if (s.ok() && e == cudaSuccess) e = cudaEventElapsedTime(&t, start, stop);
+    if (s.ok() && e == cudaSuccess && (best < 0 || t < best_time)) {
+      best = rg;
+      best_time = t;
+    }
+  }
+  if (start != nullptr) (void)cudaEventDestroy(start);
+  if (stop != nullptr) (void)cudaEventDestroy(stop);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    s = {ASC_SB_PROVIDER, std::string("CUDA SpMM autotuning failed: ") + cudaGetErrorString(e)};
+  }
+  if (s.ok() && best > 0 && plan->groups.rows_per_group != best) s = BuildRowGroups(ctx, plan, best);
+  if (!s.ok()) return Finish(ctx, s);
+  plan->use_groups = best > 0;
+  *best_ms = best_time / static_cast<float>(reps);
+  *rows_per_group = best;
+  return Finish(ctx, Status::Ok());
 }
 
 int asc_sb_plan_autotune(asc_sb_context* ctx, asc_sb_plan* plan, const asc_sb_vector* x,
@@ -1810,6 +2099,7 @@ bool ViewContext(asc_sb_context* ctx, ContextView* view) {
   view->last_error = &ctx->last_error;
   view->launches = &ctx->launches;
   view->stager = &ctx->stager;
+  view->allocator = &ctx->allocator;
   return true;
 }
 

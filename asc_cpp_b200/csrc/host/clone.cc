@@ -24,6 +24,7 @@
 
 #include "../../../include/asc_sparse_b200.h"
 #include "context_view.h"
+#include "memory.h"
 #include "validate.h"
 
 namespace ascb::host {
@@ -36,6 +37,7 @@ constexpr std::size_t kDirectBytes = std::size_t{1} << 20;
 
 class Stager {
  public:
+  explicit Stager(const Allocator& allocator) : allocator_(allocator) {}
   ~Stager() {
     {
       std::lock_guard<std::mutex> lock(m_);
@@ -48,17 +50,19 @@ class Stager {
         (void)cudaEventSynchronize(done_[b]);
         (void)cudaEventDestroy(done_[b]);
       }
-      if (buf_[b] != nullptr) (void)cudaFreeHost(buf_[b]);
+      Release(&mem_[b]);
     }
   }
 
   Status Init() {
     for (int b = 0; b < kBuffers; ++b) {
-      if (cudaHostAlloc(reinterpret_cast<void**>(&buf_[b]), kChunk, cudaHostAllocDefault) !=
-              cudaSuccess ||
-          cudaEventCreateWithFlags(&done_[b], cudaEventDisableTiming) != cudaSuccess) {
+      if (!Acquire(allocator_, kChunk, ASC_SB_PINNED_HOST, &mem_[b])) {
+        return Fail(ASC_SB_ALLOCATION, "could not allocate pinned clone staging");
+      }
+      buf_[b] = static_cast<unsigned char*>(mem_[b].ptr);
+      if (cudaEventCreateWithFlags(&done_[b], cudaEventDisableTiming) != cudaSuccess) {
         (void)cudaGetLastError();
-        return Fail(ASC_SB_ALLOCATION, "CUDA could not allocate pinned clone staging");
+        return Fail(ASC_SB_ALLOCATION, "CUDA could not create clone staging events");
       }
     }
     const unsigned hw = std::thread::hardware_concurrency();
@@ -144,6 +148,8 @@ class Stager {
   }
 
   unsigned char* buf_[kBuffers] = {};
+  Block mem_[kBuffers];
+  Allocator allocator_;
   cudaEvent_t done_[kBuffers] = {};
   bool pending_[kBuffers] = {};
   int next_ = 0;
@@ -200,6 +206,22 @@ struct CopyItem {
 // Enqueues the copies: page-locked or small sources by one DMA each, the
 // rest through the staging ring.
 Status CopyAll(const ContextView& v, const std::vector<CopyItem>& items) {
+  // the staging ring, if any copy needs it, exists before the first copy is
+  // enqueued: a failure to allocate it leaves every destination untouched
+  bool staged = false;
+  for (const CopyItem& it : items) {
+    staged = staged || (it.bytes >= kDirectBytes && !PageLocked(it.src));
+  }
+  if (staged && *v.stager == nullptr) {
+    auto* st = new (std::nothrow) Stager(*v.allocator);
+    if (st == nullptr) return Fail(ASC_SB_ALLOCATION, "clone staging allocation failed");
+    Status s = st->Init();
+    if (!s.ok()) {
+      delete st;
+      return s;
+    }
+    *v.stager = st;
+  }
   for (const CopyItem& it : items) {
     if (it.bytes == 0) continue;
     if (it.bytes < kDirectBytes || PageLocked(it.src)) {
@@ -210,16 +232,6 @@ Status CopyAll(const ContextView& v, const std::vector<CopyItem>& items) {
         return Fail(ASC_SB_MEMORY_TRANSFER, "CUDA could not enqueue a clone copy");
       }
       continue;
-    }
-    if (*v.stager == nullptr) {
-      auto* st = new (std::nothrow) Stager();
-      if (st == nullptr) return Fail(ASC_SB_ALLOCATION, "clone staging allocation failed");
-      Status s = st->Init();
-      if (!s.ok()) {
-        delete st;
-        return s;
-      }
-      *v.stager = st;
     }
     Status s = static_cast<Stager*>(*v.stager)
                    ->Copy(v.stream, static_cast<unsigned char*>(it.dst),

@@ -9,6 +9,7 @@
 #include <string>
 
 #include "../../../include/asc_sparse_b200.h"
+#include "memory.h"
 
 namespace ascb::host {
 
@@ -21,6 +22,7 @@ struct ContextView {
   std::string* last_error = nullptr;
   std::atomic<std::int64_t>* launches = nullptr;
   void** stager = nullptr;  // clone staging (clone.cc), created on first use
+  const Allocator* allocator = nullptr;  // for the context's own memory
 };
 
 // False for a null context.

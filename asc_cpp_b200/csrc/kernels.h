@@ -206,6 +206,7 @@ typedef struct ascb_trsv {
   const int64_t* order;
   const int64_t* position;
   int* status;
+  uint64_t wait_ns;  // longest wait on one dependency; 0: 2 s
 } ascb_trsv;
 size_t ascb_trsv_scratch_bytes(int64_t n, int elem_bytes);
 // exact = 1: the reference's order and rounding (DETERMINISTIC).
@@ -226,6 +227,35 @@ int ascb_trsv_analysis(void* stream, const ascb_trsv* t, void* workspace, int64_
 int ascb_spmm(void* stream, int dtype, int transpose, int exact, const ascb_csr* a,
               int64_t k, const void* b, int b_layout, int64_t ldb, void* c,
               int c_layout, int64_t ldc, double alpha, int sm_count);
+
+// ---- row-group SpMM (plan-built runs of R consecutive rows) ----
+// A plan's row groups: runs (distinct columns of each group of R rows, in
+// column order) with the rows that hold them and their values.
+typedef struct ascb_row_groups {
+  int rows_per_group;         // R: 2, 4, 8, 16 or 32
+  int64_t* group_runs;        // [groups + 1]
+  int64_t* run_col;           // [runs]
+  unsigned* run_mask;         // [runs] bit i: row g*R + i holds the column
+  unsigned* run_off;          // [runs] first value, relative to ptr[g*R]
+  void* vals;                 // [nnz] values in (group, column, row) order
+} ascb_row_groups;
+typedef struct ascb_row_groups_layout {
+  size_t group_runs, run_col, run_mask, run_off, vals, persistent;
+  size_t row_of, perm, flags, run_of, sums, total;
+} ascb_row_groups_layout;
+// Byte offsets in a 256-byte aligned block serving any R (at most
+// rows/2 + 1 groups, at most nnz runs); [persistent, total) is build scratch.
+ascb_row_groups_layout ascb_row_groups_layout_for(int64_t rows, int64_t nnz, int elem_bytes);
+// Builds the groups of CSR `a` (sorted columns) for R rows per group in
+// `base`; enqueued on the stream (integer work, deterministic).
+int ascb_row_groups_build(void* stream, const ascb_csr* a, int elem_bytes, int rows_per_group,
+                          void* base, ascb_row_groups* out, int sm_count);
+// C += alpha * A * B, row-major B and C with 16-byte aligned rows (k, ldb and
+// ldc multiples of 16 bytes / element); exact = 1: the reference's per-entry
+// update in stored order (bit-exact).
+int ascb_spmm_groups(void* stream, int dtype, int exact, const ascb_csr* a,
+                     const ascb_row_groups* rg, int64_t k, const void* b, int64_t ldb, void* c,
+                     int64_t ldc, double alpha, int sm_count);
 
 #ifdef __cplusplus
 }

@@ -36,8 +36,9 @@
 // every run.  Complex division is Smith's method (Smith, CACM 5(8), 1962) in
 // the order of the facet's DeviceArithmetic::Divide (kernels.cu:58-72).
 //
-// Every wait is bounded (2 s and a poll count); one that gives up raises an
-// abort flag that ends all other waits and records 1 in the status word.
+// Every wait is bounded (the context's wait limit, 2 s by default, and a poll
+// count); one that gives up raises an abort flag that ends all other waits
+// and records 1 in the status word.
 #include "common.cuh"
 #include "kernels.h"
 
@@ -249,7 +250,7 @@ __device__ __noinline__ void give_up(Control* ctl, int* status) {
 // Bounded spin until `ready()` holds.  False if this wait or another one gave
 // up; the caller goes on and the status word marks the result invalid.
 template <typename F>
-__device__ bool bounded_wait(F ready, Control* ctl, int* status) {
+__device__ bool bounded_wait(F ready, Control* ctl, int* status, uint64_t limit_ns) {
   if (ready()) return true;
   const uint64_t start = global_ns();
   for (uint32_t i = 1; i < kMaxPolls; ++i) {
@@ -257,11 +258,16 @@ __device__ bool bounded_wait(F ready, Control* ctl, int* status) {
     if (ready()) return true;
     if ((i & 63u) == 0u) {
       if (aborted(ctl)) return false;
-      if (global_ns() - start > kWaitNs) break;
+      if (global_ns() - start > limit_ns) break;
     }
   }
   give_up(ctl, status);
   return false;
+}
+
+// The wait limit of a solve: the context's setting, else kWaitNs.
+__device__ __forceinline__ uint64_t wait_limit(const ascb_trsv& a) {
+  return a.wait_ns != 0 ? a.wait_ns : kWaitNs;
 }
 
 __device__ __forceinline__ int64_t elem(int64_t r, int64_t j, int64_t ld, bool row_major) {
@@ -312,7 +318,7 @@ __device__ void warp_row(const ascb_trsv& a, int64_t row, T alpha, T* pub, Contr
       dep = !is_diag && !outside(a, c, row);
       if (dep) {
         T xc = A::zero();
-        bounded_wait([&] { return A::poll(pub + c, &xc); }, ctl, a.status);
+        bounded_wait([&] { return A::poll(pub + c, &xc); }, ctl, a.status, wait_limit(a));
         if (EXACT) {
           prod = A::mul(v, xc);
         } else {
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(kThreads) trsv_single(ascb_trsv a, T alpha) {
       if (idle > ASCB_TRSV_IDLE_SPIN) __nanosleep(idle > 4096 ? 256 : ASCB_TRSV_SLEEP_NS);
       if ((idle & 63u) == 0u) {
         bool stop = aborted(ctl);
-        if (!stop && (global_ns() - idle_since > kWaitNs || idle >= kMaxPolls)) {
+        if (!stop && (global_ns() - idle_since > wait_limit(a) || idle >= kMaxPolls)) {
           if (lane == 0) give_up(ctl, a.status);
           stop = true;
         }
@@ -486,7 +492,7 @@ __global__ void __launch_bounds__(kThreads) trsv_multi(ascb_trsv a, T alpha) {
             if (a.conj) v = A::conj(v);
             dep = c != row && !outside(a, c, row);
             if (dep && j0 == 0) {
-              bounded_wait([&] { return ld_acquire(ready + c) != 0u; }, ctl, a.status);
+              bounded_wait([&] { return ld_acquire(ready + c) != 0u; }, ctl, a.status, wait_limit(a));
             }
           }
           __syncwarp();
@@ -635,7 +641,7 @@ __global__ void __launch_bounds__(kThreads) trsv_levels(ascb_trsv a, int64_t* le
       if (idle > ASCB_TRSV_IDLE_SPIN) __nanosleep(idle > 4096 ? 256 : ASCB_TRSV_SLEEP_NS);
       if ((idle & 63u) == 0u) {
         bool stop = aborted(ctl);
-        if (!stop && (global_ns() - idle_since > kWaitNs || idle >= kMaxPolls)) {
+        if (!stop && (global_ns() - idle_since > wait_limit(a) || idle >= kMaxPolls)) {
           if (lane == 0) give_up(ctl, a.status);
           stop = true;
         }

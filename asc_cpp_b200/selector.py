@@ -35,7 +35,8 @@ FEATURES = 12
 HIDDEN = 64
 # candidate variants, in output order: (variant, lanes)
 VARIANTS: list[tuple[int, int]] = [(int(Variant.kWarpTiles), 0), (int(Variant.kMergePath), 0)] + \
-    [(int(Variant.kVector), lanes) for lanes in (1, 2, 4, 8, 16, 32)]
+    [(int(Variant.kVector), lanes) for lanes in (1, 2, 4, 8, 16, 32)] + \
+    [(int(Variant.kRowSplit), 0)]
 DEFAULT = 0  # the library's default variant (WARP_TILES) is output 0
 FAMILIES = ("banded", "powerlaw", "blockdiag", "uniform")
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "selector_weights.npz")
@@ -197,6 +198,37 @@ def install(context: sc.SparseCudaContext, path: str = WEIGHTS) -> None:
         lanes.ctypes.data))
 
 
+DEFAULT_INC = os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc", "host",
+                           "selector_default.inc")
+
+
+def export_c(path: str = WEIGHTS, out: str = DEFAULT_INC) -> str:
+    """Writes the weights as the C++ tables the library installs on every new
+    context (csrc/host/selector_default.inc)."""
+    w = np.load(path)
+    params = np.asarray(w["params"], np.float32)
+    variants = np.asarray(w["variants"], np.int32)
+    lanes = np.asarray(w["lanes"], np.int32)
+    assert params.size == param_count(variants.size)
+    lines = ["// Trained variant selector installed on every new context.  Generated by",
+             "// `python -m asc_cpp_b200.selector export-c` from selector_weights.npz;",
+             "// do not edit.",
+             f"constexpr int kDefaultSelectorOutputs = {variants.size};",
+             "constexpr int32_t kDefaultSelectorVariants[] = {" +
+             ", ".join(str(int(v)) for v in variants) + "};",
+             "constexpr int32_t kDefaultSelectorLanes[] = {" +
+             ", ".join(str(int(v)) for v in lanes) + "};",
+             "constexpr float kDefaultSelectorParams[] = {"]
+    vals = [np.format_float_scientific(v, unique=True) + "f" if np.isfinite(v) else "0.0f"
+            for v in params.astype(np.float32)]
+    for i in range(0, len(vals), 6):
+        lines.append("    " + ", ".join(vals[i:i + 6]) + ",")
+    lines.append("};")
+    with open(out, "w") as f:
+        f.write("\n".join(lines) + "\n")
+    return out
+
+
 # ---- synthetic families (generated on the GPU) ----------------------------------
 
 def _csr_from_keys(keys: torch.Tensor, n: int, dtype, gen) -> sc.CudaCsrArray:
@@ -327,7 +359,13 @@ def main() -> None:
     t.add_argument("--out", required=True)
     t.add_argument("--train-count", type=int, default=1600)
     t.add_argument("--epochs", type=int, default=3000)
+    e = sub.add_parser("export-c")
+    e.add_argument("--weights", default=WEIGHTS)
+    e.add_argument("--out", default=DEFAULT_INC)
     a = ap.parse_args()
+    if a.cmd == "export-c":
+        print(export_c(a.weights, a.out))
+        return
     if a.cmd == "collect":
         np.savez_compressed(a.out, **collect(a.count, a.seed, nnz_cap=a.nnz_cap))
         return

@@ -450,6 +450,20 @@ class CsrPlan:
         self.context.check(self.context._lib.asc_sb_plan_refresh_values(
             self.context.handle, self._h))
 
+    def spmm_autotune(self, alpha: float, b: "DenseMatrixView", c: "DenseMatrixView",
+                      reps: int = 5) -> tuple[float, int]:
+        """Times the SpMM kernels on these operands (C accumulates) and keeps
+        the fastest; returns (ms per product, rows per group, 0 = row by row).
+        Needs a plan created with PLAN_ROW_GROUPS."""
+        bd, cd = b.describe(), c.describe()
+        bd.writable = 0
+        ms = ctypes.c_float()
+        rg = ctypes.c_int32()
+        self.context.check(self.context._lib.asc_sb_plan_spmm_autotune(
+            self.context.handle, self._h, float(alpha), ctypes.byref(bd), ctypes.byref(cd),
+            reps, ctypes.byref(ms), ctypes.byref(rg)))
+        return ms.value, rg.value
+
     def csr_spmv(self, alpha: float, x: CudaStridedVectorView, beta: float,
                  y: CudaStridedVectorView) -> None:
         xd, yd = x.describe(), y.describe()

@@ -247,6 +247,78 @@ def cusparse_leg(a, A, x, stream, bytes_step):
             "note": "library comparison on the same arrays (torch CSR mat-vec), not the product"}
 
 
+def selector_leg(count=40, seed=5, max_rows=1_000_000, reps=10):
+    """The learned selector on the drop-in path, re-timed on this GPU: `count`
+    matrices of the training families drawn with a seed the selector never saw
+    (training used seed 4), each multiplied through CudaCsrSpmv (the C ABI
+    entry a reference caller reaches) in BACKEND_DEFAULT mode with the shipped
+    selector installed (the context's default), against the default variant
+    forced and against exhaustive autotuning (every candidate timed)."""
+    import ctypes
+    import torch
+    from asc_cpp_b200 import selector as sel
+    from asc_cpp_b200 import sparse_cuda as sc
+    from asc_cpp_b200._abi import Determinism, Variant
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.Stream(device=dev)
+    timed = _timer(stream, reps, 3)
+    ctx = sc.SparseCudaContext.Create(0, stream=stream, determinism=Determinism.kBackendDefault)
+    rng = np.random.default_rng(seed)
+    variants = np.array([v for v, _ in sel.VARIANTS], np.int32)
+    lanes = np.array([l for _, l in sel.VARIANTS], np.int32)
+    rows = []
+    for i in range(count):
+        family = sel.FAMILIES[i % len(sel.FAMILIES)]
+        n = int(np.exp(rng.uniform(np.log(10_000), np.log(max_rows))))
+        dtype = torch.float64 if rng.random() < 0.5 else torch.float32
+        with torch.cuda.stream(stream):
+            m = sel.family_matrix(family, n, rng, dtype, 20_000_000, dev)
+            x = (torch.rand(m.columns, device=dev, dtype=torch.float64) * 2 - 1).to(dtype)
+            y = torch.zeros(m.rows, dtype=dtype, device=dev)
+        stream.synchronize()
+        xv = sc.CudaStridedVectorView(x, m.columns, writable=False)
+        yv = sc.CudaStridedVectorView(y, m.rows)
+        need = sc.CudaCsrSpmvWorkspaceSize(ctx, m, xv, yv)
+        ws = torch.empty(max(need, 1), dtype=torch.uint8, device=dev)
+
+        def product():
+            sc.CudaCsrSpmv(ctx, 1.0, m, xv, 0.0, yv, ws, need)
+        ctx.set_variant(Variant.kWarpTiles, 0)
+        t_default = timed(product)
+        ctx.set_variant(Variant.kAuto, 0)
+        product()  # first sight of this matrix: the selection is enqueued
+        stream.synchronize()
+        t_pick = timed(product)  # the pick, once it has landed
+        plan = sc.CsrPlan(ctx, m)  # the same selector on a plan: which variant it is
+        v, l = ctypes.c_int32(), ctypes.c_int32()
+        ctx.check(ctx._lib.asc_sb_plan_variant(plan.handle, ctypes.byref(v), ctypes.byref(l)))
+        ms = np.zeros(len(variants), np.float32)
+        xd, yd = xv.describe(), yv.describe()
+        xd.writable = 0
+        ctx.check(ctx._lib.asc_sb_plan_autotune(ctx.handle, plan.handle, ctypes.byref(xd),
+                                                ctypes.byref(yd), len(variants),
+                                                variants.ctypes.data, lanes.ctypes.data, reps,
+                                                ms.ctypes.data))
+        plan.close()
+        rows.append((family, m.rows, m.nnz, t_default, t_pick, float(ms.min()),
+                     (int(v.value), int(l.value))))
+        del m, x, y, ws
+    ctx.close()
+    d = np.array([r[3] for r in rows])
+    p = np.array([r[4] for r in rows])
+    b = np.array([r[5] for r in rows])
+    best = np.minimum(b, np.minimum(d, p))
+    return {"matrices": count, "seed": seed, "path": "CudaCsrSpmv (asc_sb_csr_spmv), "
+            "BACKEND_DEFAULT, shipped selector installed at context creation",
+            "geomean_speedup_vs_default": round(float(np.exp(np.log(d / p).mean())), 3),
+            "total_time_speedup_vs_default": round(float(d.sum() / p.sum()), 3),
+            "geomean_slowdown_vs_exhaustive": round(float(np.exp(np.log(p / best).mean())), 3),
+            "within_10pct_of_exhaustive": round(float((p <= 1.1 * best).mean()), 3),
+            "picks": {f"{v}/{l}": sum(1 for r in rows if r[6] == (v, l))
+                      for v, l in sorted({r[6] for r in rows})}}
+
+
 def cpu_baseline_sample(a, x):
     """The reference's serial CPU SpMV (1 core) on a bounded row sample."""
     from oracle import Reference, Restatement, build_oracle
@@ -442,6 +514,7 @@ def run_gpu(args, rank, world):
     # comparison only (never the product): cuSPARSE through torch's CSR
     # mat-vec on the same arrays, int64 indices
     comparison = cusparse_leg(a_h, A, x, stream, bytes_step) if rank == 0 else None
+    selection = selector_leg() if rank == 0 and world == 1 and not args.no_selector else None
     peak, peak_kind = _peaks()
     traffic = _traffic_record().get(WORKLOAD)
     out = None
@@ -476,6 +549,7 @@ def run_gpu(args, rank, world):
             "detail_gbs": {k: round(v, 2) for k, v in detail.items()},
             "error_vs_fp64_oracle": error,
             "comparison": comparison,
+            "selector_drop_in": selection,
         }
     plan.close()
     ctx.close()
@@ -854,6 +928,8 @@ def main():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-selector", action="store_true",
+                   help="skip the selector leg of the headline run")
     p.add_argument("--probe", default=None,
                    help="profiling aid: run 3 launches of one variant and exit")
     p.add_argument("--workload", default=WORKLOAD,

@@ -173,6 +173,32 @@ ASC_SB_API int asc_sb_context_set_determinism(asc_sb_context* context,
  * sums are combined in a fixed order, so results repeat run to run. */
 ASC_SB_API int asc_sb_context_set_variant(asc_sb_context* context,
                                           int32_t variant, int32_t lanes);
+/* Allocator for the memory a context allocates for itself after creation:
+ * the scratch of triangular solves without a plan (device; it grows to the
+ * largest solve), the variant selector's parameters (device) and the clone
+ * staging buffers (pinned host).  `allocate` returns NULL on failure; the
+ * call that needed the memory then returns ASC_SB_ALLOCATION without having
+ * touched its outputs, and the context stays usable.  `release` (may be
+ * NULL: blocks are then never returned) gets back every block `allocate`
+ * gave, with the same size and space, when the context no longer needs it.
+ * Passing NULL for `allocate` restores cudaMalloc / cudaHostAlloc.  Lets a
+ * host application that owns all device memory, or a test that fails chosen
+ * allocations, serve these requests.  No counterpart in the reference (its
+ * provider allocates only from the caller's MemoryResource, in clones). */
+typedef void* (*asc_sb_allocate_fn)(void* user, size_t bytes, int32_t memory_space);
+typedef void (*asc_sb_deallocate_fn)(void* user, void* pointer, size_t bytes,
+                                     int32_t memory_space);
+ASC_SB_API int asc_sb_context_set_allocator(asc_sb_context* context,
+                                            asc_sb_allocate_fn allocate,
+                                            asc_sb_deallocate_fn release, void* user);
+/* Longest time a kernel of this context spins on a value another warp has
+ * not published yet (the dependencies of triangular solves) before it gives
+ * up: the call's results are then invalid, the device status word
+ * (asc_sb_context_device_status) becomes 1, every other wait of the launch
+ * ends at once, and the kernel returns, leaving the context usable.
+ * 0 restores the default, 2 s.  No counterpart in the reference. */
+ASC_SB_API int asc_sb_context_set_wait_limit(asc_sb_context* context,
+                                             int64_t nanoseconds);
 ASC_SB_API void* asc_sb_context_stream(const asc_sb_context* context);
 ASC_SB_API int asc_sb_context_synchronize(asc_sb_context* context);
 /* Message of the most recent failure on this context ("" if none). */
@@ -347,7 +373,16 @@ ASC_SB_API int asc_sb_clone_indexed(asc_sb_context* context,
 /* ASC_SB_PLAN_TRIANGULAR adds the ready flags of triangular solves
  * (asc_sb_plan_triangular_solve); solves through one plan must be ordered
  * (one stream). */
-enum { ASC_SB_PLAN_TRANSPOSE = 1, ASC_SB_PLAN_TRIANGULAR = 2 };
+/* ASC_SB_PLAN_ROW_GROUPS (CSR, float or double) merges the column lists of
+ * every R consecutive rows (R = 8 at creation; asc_sb_plan_spmm_autotune may
+ * choose another) into runs -- one per distinct column, with the rows that
+ * hold it -- so that asc_sb_plan_standard_spmm (op = none, row-major B and C
+ * with 16-byte aligned rows) loads each row of B once per run and applies it
+ * to all of the run's rows.  Each row still adds its entries in stored
+ * order: DETERMINISTIC results stay bit-identical to the reference.  The
+ * groups are used when they share B rows (at least 1.25 entries per run) or
+ * when the autotuner found them faster. */
+enum { ASC_SB_PLAN_TRANSPOSE = 1, ASC_SB_PLAN_TRIANGULAR = 2, ASC_SB_PLAN_ROW_GROUPS = 4 };
 typedef struct asc_sb_plan asc_sb_plan;
 ASC_SB_API int asc_sb_plan_workspace_size(asc_sb_context* context,
                                           const asc_sb_sparse* matrix,
@@ -381,7 +416,8 @@ ASC_SB_API int asc_sb_plan_standard_spmv(asc_sb_context* context,
  * FP32 operands split into three TF32 products), within
  * |c - c_exact| <= (n + 64) 2^-22 |alpha| sum_k |a_k b_k| + 2^-23 |c0| per
  * output (n = stored entries of the row). */
-enum { ASC_SB_PLAN_HAS_TRANSPOSE = 1, ASC_SB_PLAN_HAS_BLOCKS16 = 2 };
+enum { ASC_SB_PLAN_HAS_TRANSPOSE = 1, ASC_SB_PLAN_HAS_BLOCKS16 = 2,
+       ASC_SB_PLAN_HAS_ROW_GROUPS = 4 /* SpMM runs through the row groups */ };
 ASC_SB_API int asc_sb_plan_properties(const asc_sb_plan* plan,
                                       int32_t* properties);
 /* Standard SpMM through a plan: same contract as asc_sb_standard_spmm, with
@@ -392,6 +428,18 @@ ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
                                          double alpha_real, double alpha_imag,
                                          const asc_sb_dense* input,
                                          const asc_sb_dense* output);
+/* SpMM autotuner of a plan created with ASC_SB_PLAN_ROW_GROUPS: times, on
+ * these operands (C += alpha * A * B, `reps` products each plus one warm-up,
+ * CUDA events on the context stream), the row-by-row kernel and the row-group
+ * kernel with R = 2, 4, 8, 16 and 32 rows per group (k-tile and lanes per row
+ * follow from R and k), keeps the fastest for the plan's later products and
+ * returns its time per product and R (0: row by row).  The products run for
+ * real, so C accumulates.  No counterpart in the reference. */
+ASC_SB_API int asc_sb_plan_spmm_autotune(asc_sb_context* context,
+                                         asc_sb_plan* plan, double alpha,
+                                         const asc_sb_dense* input,
+                                         const asc_sb_dense* output, int32_t reps,
+                                         float* best_ms, int32_t* rows_per_group);
 
 /* Triangular solve through a plan created with ASC_SB_PLAN_TRIANGULAR: same
  * contract as asc_sb_standard_triangular_solve on the plan's matrix; op !=
