@@ -205,6 +205,86 @@ __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
   }
 }
 
+// EXACT tile: the window's products are formed in parallel (8 contiguous
+// positions per lane, as in the contracted tile) and staged in shared memory;
+// then lane k, which holds row r0 + k's bounds, adds that row's products in
+// stored order from shared memory -- the serial reference's chain, with every
+// row of the tile summed at once by its own lane.  A last row that runs past
+// the window continues in rounds of 256 products (all lanes form them, its
+// lane adds them).  No per-position bitmap, ranks or lane-to-lane hand-over:
+// the instruction count per tile follows the longest row, not the number of
+// lane boundaries the rows cross.
+template <typename T, bool STANDARD, bool UNIT, bool V32>
+__device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
+                                           const int64_t* __restrict__ idx,
+                                           const T* __restrict__ val, const T* __restrict__ x,
+                                           int64_t incx, T* __restrict__ y, int64_t incy,
+                                           T alpha, T beta, int64_t r0, int nr, int64_t rb,
+                                           int64_t re) {
+  constexpr int64_t kAlign = V32 ? (sizeof(T) == 8 ? 4 : 8) : (sizeof(T) == 8 ? 2 : 4);
+  const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
+  const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
+  const int64_t a0 = base / kAlign * kAlign;
+  const int lo = static_cast<int>(base - a0);
+  const int window = static_cast<int>(span < kItems - lo ? span : kItems - lo);
+  const int lim = lo + window;
+  const bool ends_here = span <= window;
+
+  const int p0 = kPer * lane;
+  const int vlo = lo - p0 < 0 ? 0 : (lo - p0 > kPer ? kPer : lo - p0);
+  const int vhi = lim - p0 < 0 ? 0 : (lim - p0 > kPer ? kPer : lim - p0);
+  const uint32_t vmask = ((1u << vhi) - 1u) & ~((1u << vlo) - 1u);
+  T p[kPer];
+  lane_products<T, true, STANDARD, UNIT, V32>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
+                                              alpha);
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = p[k];
+  __syncwarp();
+
+  const bool mine = lane < nr;
+  const bool carries = !ends_here && lane == nr - 1;  // the row that runs on
+  T acc = T(0);
+  T* yp = mine ? &at<UNIT>(y, r0 + lane, incy) : nullptr;
+  if (mine) {
+    if (STANDARD) acc = *yp;
+    const int s0 = static_cast<int>(rb - a0);
+    const int e0 = static_cast<int>(re - a0 < lim ? re - a0 : lim);
+    int q = s0;
+    for (; q + 4 <= e0; q += 4) {
+      const T u0 = w.prod[q], u1 = w.prod[q + 1], u2 = w.prod[q + 2], u3 = w.prod[q + 3];
+      acc = add_rn(add_rn(add_rn(add_rn(acc, u0), u1), u2), u3);
+    }
+    for (; q < e0; ++q) acc = add_rn(acc, w.prod[q]);
+    if (!carries) *yp = finish<true, STANDARD>(acc, alpha, beta, yp);
+  }
+  if (!ends_here) {
+    // the last row past the window: rounds of 256 products, added in stored
+    // order by its lane (the window ends on an aligned position, a0 + 256)
+    for (int64_t q0 = base + window; q0 < base + span; q0 += kItems) {
+      const int64_t rem = base + span - q0;
+      const int cnt = static_cast<int>(rem < kItems ? rem : kItems);
+      const int hi = cnt - p0 < 0 ? 0 : (cnt - p0 > kPer ? kPer : cnt - p0);
+      T q[kPer];
+      __syncwarp();  // the previous round's products have been read
+      lane_products<T, true, STANDARD, UNIT, V32>(q, (1u << hi) - 1u, idx + (q0 + p0),
+                                                  val + (q0 + p0), x, incx, alpha);
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = q[k];
+      __syncwarp();
+      if (carries) {
+        int k = 0;
+        for (; k + 4 <= cnt; k += 4) {
+          const T u0 = w.prod[k], u1 = w.prod[k + 1], u2 = w.prod[k + 2], u3 = w.prod[k + 3];
+          acc = add_rn(add_rn(add_rn(add_rn(acc, u0), u1), u2), u3);
+        }
+        for (; k < cnt; ++k) acc = add_rn(acc, w.prod[k]);
+      }
+    }
+    if (carries) *yp = finish<true, STANDARD>(acc, alpha, beta, yp);
+  }
+  __syncwarp();  // the product buffer is rewritten by the next tile
+}
+
 // One tile: rows r0 .. r0 + nr - 1 (nr >= 1), whose ptr entries lane k holds
 // as rb = ptr[r0 + k], re = ptr[r0 + k + 1] (k < nr).  Shared by the
 // single-matrix and the batched kernels.
@@ -214,6 +294,11 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
                                          int64_t incx, T* __restrict__ y, int64_t incy, T alpha,
                                          T beta, int64_t r0, int nr, int64_t rb, int64_t re,
                                          const SplitBlock* split = nullptr) {
+  if constexpr (EXACT) {
+    exact_tile<T, STANDARD, UNIT, V32>(w, lane, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
+                                       rb, re);
+    return;
+  }
   const unsigned lt_mask = (1u << lane) - 1u;
   // window start alignment: each lane's 8 values and 8 indices start on a
   // 16-byte (V32: 32-byte) boundary (the arrays are aligned so, checked by

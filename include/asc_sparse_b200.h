@@ -6,8 +6,9 @@
  * cuda.h, src/sparse/cuda/operations.cc, src/sparse/cuda/kernels.cu).  Every
  * entry point takes plain pointers, sizes and enums -- no C++ or torch types --
  * so that the reference's exported `internal_sparse_cuda::*Erased` functions
- * can forward to it one-for-one, and so that ctypes,
- * cgo or any other FFI can bind it directly.
+ * can forward to it one-for-one (asc_cpp_b200/binding/sparse_cuda_provider.cc
+ * is that forwarding layer), and so that ctypes, cgo or any other FFI can
+ * bind it directly.
  *
  * Semantics mirror the reference exactly:
  *   - enum values are numerically identical to the reference enums;
