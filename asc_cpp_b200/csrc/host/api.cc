@@ -85,6 +85,8 @@ struct Partitions {
   const std::int64_t* merge_bounds = nullptr;  // ascb_merge_bounds pairs
   std::int64_t n_merge = 0;
   void* split = nullptr;  // row-split block (ascb_split_bytes(nnz, 256) bytes)
+  const std::int64_t* seg_tiles = nullptr;  // the segmented kernel's own row tiles
+  std::int64_t n_seg = 0;
 };
 
 struct asc_sb_plan {
@@ -213,6 +215,12 @@ std::int64_t WarpTiles(std::int64_t rows, std::int64_t nnz) {
 std::size_t WarpTileBytes(std::int64_t rows, std::int64_t nnz) {
   return RoundUp(static_cast<std::size_t>(WarpTiles(rows, nnz) + 1) * 8, 256);
 }
+std::int64_t SegTiles(std::int64_t rows, std::int64_t nnz) {
+  return ascb_row_tile_count(rows, nnz, ascb_warp_tile_items(), ascb_seg_tile_row_weight());
+}
+std::size_t SegTileBytes(std::int64_t rows, std::int64_t nnz) {
+  return RoundUp(static_cast<std::size_t>(SegTiles(rows, nnz) + 1) * 8, 256);
+}
 std::size_t MergeBoundBytes(std::int64_t rows, std::int64_t nnz) {
   return RoundUp(static_cast<std::size_t>(ascb_merge_tiles(rows, nnz) + 1) * 16, 256);
 }
@@ -305,22 +313,28 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
     // no partition buffer at all (zero-workspace calls): warp tiles with
     // in-kernel bound search
   }
-  const std::int64_t tiles = WarpTiles(a.rows, a.nnz);
-  const std::int64_t* tiles_ptr = planned != nullptr ? planned->warp_tiles : nullptr;
+  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) run the register-
+  // segmented kernel, which needs 16-byte aligned index and value arrays, on
+  // its own row tiles (up to 128 rows each); otherwise the scalar-load warp
+  // kernel, with the same numerics, on tiles of at most 32 rows.  Either
+  // partition fits the front of the workspace (fewer tiles for the smaller
+  // row weight).
+  const bool seg_aligned =
+      ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
+       static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
+  const std::int64_t weight =
+      seg_aligned ? ascb_seg_tile_row_weight() : ascb_warp_tile_row_weight();
+  const std::int64_t tiles = ascb_row_tile_count(a.rows, a.nnz, ascb_warp_tile_items(), weight);
+  const std::int64_t* tiles_ptr =
+      planned != nullptr ? (seg_aligned ? planned->seg_tiles : planned->warp_tiles) : nullptr;
   if (tiles_ptr == nullptr && scratch != nullptr) {
     Status s = Launched(ctx,
-                        ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
-                                       ascb_warp_tile_row_weight(), scratch, tiles),
+                        ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(), weight, scratch,
+                                       tiles),
                         "CUDA could not launch the row-tile partition kernel");
     if (!s.ok()) return s;
     tiles_ptr = scratch;
   }
-  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) run the register-
-  // segmented kernel, which needs 16-byte aligned index and value arrays;
-  // otherwise the scalar-load warp kernel with the same numerics.
-  const bool seg_aligned =
-      ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
-       static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
   if (choice.variant == ASC_SB_VARIANT_ROW_SPLIT && seg_aligned) {
     // the split block lives in the plan, or after the tile bounds in the
     // caller's workspace; without either (the standard path without a plan)
@@ -334,15 +348,15 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
       const std::int64_t rounds = choice.lanes > 0 ? choice.lanes : kSplitRounds;
       return Launched(ctx,
                       ascb_spmv_split(ctx->stream, dtype, form, &a, alpha, beta, &x, &y,
-                                      tiles_ptr, tiles, rounds * ascb_warp_tile_items(), block,
-                                      ctx->sm_count),
+                                      tiles_ptr, tiles, weight, rounds * ascb_warp_tile_items(),
+                                      block, ctx->sm_count),
                       "CUDA could not launch the row-split SpMV kernels");
     }
   }
   if (seg_aligned) {
     return Launched(ctx,
-                    ascb_spmv_seg(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
-                                  tiles_ptr, tiles, ctx->sm_count),
+                    ascb_spmv_seg_w(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
+                                    tiles_ptr, tiles, weight, ctx->sm_count),
                     "CUDA could not launch the segmented SpMV kernel");
   }
   return Launched(ctx,
@@ -361,17 +375,27 @@ Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* bu
   out->warp_tiles = warp;
   out->merge_bounds = merge;
   out->split = buffer + WarpTileBytes(a.rows, a.nnz) + MergeBoundBytes(a.rows, a.nnz);
+  auto* seg = reinterpret_cast<std::int64_t*>(static_cast<unsigned char*>(out->split) +
+                                              SplitBlockBytes(a.nnz));
+  out->seg_tiles = seg;
+  out->n_seg = SegTiles(a.rows, a.nnz);
   if (a.rows == 0) return Status::Ok();
   Status s = Launched(ctx,
                       ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
                                      ascb_warp_tile_row_weight(), warp, out->n_warp),
                       "CUDA could not launch the row-tile partition kernel");
   if (!s.ok()) return s;
+  s = Launched(ctx,
+               ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(), ascb_seg_tile_row_weight(),
+                              seg, out->n_seg),
+               "CUDA could not launch the row-tile partition kernel");
+  if (!s.ok()) return s;
   return Launched(ctx, ascb_merge_bounds(ctx->stream, &a, merge, out->n_merge),
                   "CUDA could not launch the merge partition kernel");
 }
 std::size_t PartitionBytes(std::int64_t rows, std::int64_t nnz) {
-  return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz) + SplitBlockBytes(nnz);
+  return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz) + SplitBlockBytes(nnz) +
+         SegTileBytes(rows, nnz);
 }
 
 std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
@@ -971,6 +995,47 @@ ascb_csr TransposedCsr(const asc_sb_plan& plan) {
   return t;
 }
 
+Status SolveScratch(asc_sb_context* ctx, std::size_t bytes, unsigned char** out);
+
+// The transposed structure of the CSR arrays `a`, built on the stream into the
+// context's scratch buffer (which grows, after a stream drain, to the largest
+// request): the deterministic transposed products of callers without a plan.
+// Stable by source row, so a stored-order kernel on it adds each output's
+// terms in the reference's order (blas.h:1241-1256).
+Status TransposedInScratch(asc_sb_context* ctx, const ascb_csr& a, std::size_t element,
+                           ascb_csr* out) {
+  const std::int64_t nnz = a.nnz;
+  std::size_t total = 0;
+  const std::size_t t_ptr = total;
+  total += RoundUp(static_cast<std::size_t>(a.cols + 1) * 8, 256);
+  const std::size_t t_idx = total;
+  total += EntryBytes(nnz, 8);
+  const std::size_t t_perm = total;
+  total += EntryBytes(nnz, 8);
+  const std::size_t t_val = total;
+  total += EntryBytes(nnz, element);
+  const std::size_t sort = total;
+  total += RoundUp(ascb_sort_workspace_bytes(nnz, a.cols), 256);
+  const std::size_t outer_of = total;
+  total += EntryBytes(nnz, 8);
+  unsigned char* base = nullptr;
+  Status s = SolveScratch(ctx, total, &base);
+  if (!s.ok()) return s;
+  auto* tp = reinterpret_cast<std::int64_t*>(base + t_ptr);
+  auto* ti = reinterpret_cast<std::int64_t*>(base + t_idx);
+  s = BuildTransposed(ctx, a, element, tp, ti, reinterpret_cast<std::int64_t*>(base + t_perm),
+                      base + t_val, base + sort, reinterpret_cast<std::int64_t*>(base + outer_of));
+  if (!s.ok()) return s;
+  *out = ascb_csr{};
+  out->rows = a.cols;
+  out->cols = a.rows;
+  out->nnz = a.nnz;
+  out->ptr = tp;
+  out->idx = ti;
+  out->val = base + t_val;
+  return Status::Ok();
+}
+
 // Runs y += alpha * op(A) x.  The stored arrays are read as a CSR matrix `a`
 // (for CSC: the CSR of A^T); `transposed` says whether the product needs the
 // transpose of those arrays.
@@ -985,13 +1050,13 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
   if (!RealKind(m.element_kind)) {
     const bool planned = transposed && plan != nullptr && plan->t_ptr != nullptr;
     const bool exact = ctx->determinism == ASC_SB_DETERMINISTIC;
-    if (transposed && !planned && exact) {
-      return Fail(ASC_SB_INVALID_STATE,
-                  "A deterministic transposed product needs a plan created with "
-                  "ASC_SB_PLAN_TRANSPOSE");
+    ascb_csr rows_of_op = planned ? TransposedCsr(*plan) : a;
+    const bool built = transposed && !planned && exact;
+    if (built) {
+      Status s = TransposedInScratch(ctx, a, ascb::host::ElementBytes(m.element_kind), &rows_of_op);
+      if (!s.ok()) return s;
     }
-    const ascb_csr rows_of_op = planned ? TransposedCsr(*plan) : a;
-    const int mode = transposed && !planned ? 2 : (exact ? 1 : 0);
+    const int mode = transposed && !planned && !built ? 2 : (exact ? 1 : 0);
     return Launched(ctx,
                     ascb_complex_spmv(ctx->stream, dtype, mode,
                                       op == ASC_SB_OP_CONJUGATE_TRANSPOSE ? 1 : 0, &rows_of_op,
@@ -1011,9 +1076,13 @@ Status RunStandardSpmv(asc_sb_context* ctx, const asc_sb_plan* plan,
                   &plan->t_part);
   }
   if (ctx->determinism == ASC_SB_DETERMINISTIC) {
-    return Fail(ASC_SB_INVALID_STATE,
-                "A deterministic transposed product needs a plan created with "
-                "ASC_SB_PLAN_TRANSPOSE");
+    // the reference's order without a plan: the transposed structure in the
+    // context's scratch, rebuilt for this call
+    ascb_csr t{};
+    Status s = TransposedInScratch(ctx, a, ascb::host::ElementBytes(m.element_kind), &t);
+    if (!s.ok()) return s;
+    return RunCsr(ctx, Choose(ctx, m), ASCB_STANDARD, t, dtype, alpha, 0.0, xv, yv, nullptr,
+                  nullptr);
   }
   return Launched(ctx, ascb_spmv_scatter(ctx->stream, dtype, &a, alpha, &xv, &yv, ctx->sm_count),
                   "CUDA could not launch the scatter SpMV kernel");
@@ -1086,13 +1155,17 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
   }
   const bool csc = m->format == ASC_SB_CSC;
   const bool transposed = (op != ASC_SB_OP_NONE) != csc;
-  const bool planned = transposed && plan != nullptr && plan->t_ptr != nullptr;
+  bool planned = transposed && plan != nullptr && plan->t_ptr != nullptr;
+  ascb_csr a = planned ? TransposedCsr(*plan) : AsCsr(*m, csc);
   if (transposed && !planned && ctx->determinism == ASC_SB_DETERMINISTIC) {
-    return Fail(ASC_SB_INVALID_STATE,
-                "A deterministic transposed SpMM needs a plan created with "
-                "ASC_SB_PLAN_TRANSPOSE");
+    // the reference's order without a plan: the transposed structure in the
+    // context's scratch, rebuilt for this call
+    ascb_csr t{};
+    s = TransposedInScratch(ctx, a, ascb::host::ElementBytes(m->element_kind), &t);
+    if (!s.ok()) return s;
+    a = t;
+    planned = true;
   }
-  const ascb_csr a = planned ? TransposedCsr(*plan) : AsCsr(*m, csc);
   if (!transposed && !csc && plan != nullptr && plan->block16 &&
       m->element_kind == ASC_SB_FLOAT && ctx->determinism != ASC_SB_DETERMINISTIC &&
       ctx->variant == ASC_SB_VARIANT_AUTO && b->layout == ASC_SB_ROW_MAJOR &&

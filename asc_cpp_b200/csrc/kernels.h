@@ -85,6 +85,14 @@ int ascb_spmv_seg_alignment(void);
 int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
                   double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
                   int64_t ntiles, int sm_count);
+// The same over row tiles of weight `weight`: ascb_warp_tile_row_weight() (at
+// most 32 rows per tile, as ascb_spmv_seg) or ascb_seg_tile_row_weight() (the
+// segmented kernel's own partition: more rows per tile, so more of each
+// window holds nonzeros when rows are short).
+int64_t ascb_seg_tile_row_weight(void);
+int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
+                    double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
+                    int64_t ntiles, int64_t weight, int sm_count);
 // Row split (contracted only): like ascb_spmv_seg with exact = 0, except that
 // a row running more than split_min (>= 256) positions past its tile's window
 // is finished by a second kernel whose warps take its tail in 256-position
@@ -94,7 +102,8 @@ int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* 
 size_t ascb_split_bytes(int64_t nnz, int64_t split_min);
 int ascb_spmv_split(void* stream, int dtype, int form, const ascb_csr* a, double alpha,
                     double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
-                    int64_t ntiles, int64_t split_min, void* block, int sm_count);
+                    int64_t ntiles, int64_t weight, int64_t split_min, void* block,
+                    int sm_count);
 // ---- batched compat SpMV: many independent CSR matrices, one launch ----
 // One matrix of a batch, as the persistent kernel reads it (device table).
 typedef struct ascb_batch_item {

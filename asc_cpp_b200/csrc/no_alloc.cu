@@ -21,9 +21,11 @@
 //     ordering between them -- race on it and may compute wrong results;
 //   * the array keeps whatever the last call wrote; each call overwrites every
 //     entry it reads before reading it, so nothing needs clearing;
-//   * it always runs the default kernel (the variant forced on a context with
-//     asc_sb_context_set_variant does not apply), so its results equal
-//     asc_sb_csr_spmv's when the context's variant is AUTO;
+//   * it always runs the default kernel (neither a variant forced with
+//     asc_sb_context_set_variant nor a selector pick applies): its results
+//     equal asc_sb_csr_spmv's bit for bit in DETERMINISTIC mode, and in
+//     BACKEND_DEFAULT mode whenever that call also runs the default kernel
+//     (both meet the same bound);
 //   * the first call on each device looks up the array's device address
 //     (cudaGetSymbolAddress) and keeps it.  Make that first call before any
 //     stream capture starts on that device.  A cudaDeviceReset invalidates

@@ -30,7 +30,18 @@ namespace {
 constexpr int kWarpsPerCta = 4;
 constexpr int kThreads = kWarpsPerCta * 32;
 constexpr int kItems = 256;        // weighted items per tile (= positions)
-constexpr int kRowWeight = kItems / 32;
+constexpr int kRowWeight = kItems / 32;  // the warp-tile partition: at most 32 rows
+// Row weight of the segmented kernel's own partition (ascb_seg_tile_row_weight):
+// a tile holds at most kItems / weight rows, so a smaller weight leaves more of
+// each 256-position window to nonzeros on matrices with short rows.
+#ifndef ASCB_SEG_ROW_WEIGHT
+#define ASCB_SEG_ROW_WEIGHT 2
+#endif
+constexpr int kSegWeight = ASCB_SEG_ROW_WEIGHT;
+constexpr int kMaxRowsPerLane = kRowWeight / kSegWeight;  // rows per lane in a tile
+constexpr int kMaxRows = 32 * kMaxRowsPerLane;
+static_assert(kRowWeight % kSegWeight == 0 && kMaxRowsPerLane >= 1 && kMaxRowsPerLane <= 8,
+              "the segmented kernel's row weight divides 8");
 constexpr int kPer = 8;            // contiguous positions per lane
 constexpr int kChunk = 32;         // tile bounds cached per warp
 constexpr int kMaxDevices = 64;
@@ -66,9 +77,8 @@ constexpr unsigned long long kChunkMask = (1ull << 40) - 1;
 template <typename T>
 struct SegSmem {
   uint32_t bits[kItems / 32 + 1];  // row-start bitmap of positions 0..256
-  int rowid[33];                   // k-th nonempty row of the tile -> lane
+  int16_t rowid[kMaxRows + 1];     // k-th nonempty row of the tile -> its offset
   int64_t bnd[kChunk + 1];         // first row of tiles c0 .. c0 + kChunk
-  T yinit[33];                     // exact standard form: y of the k-th row
   T prod[kItems];                  // exact form: products of a long row's tail
 };
 
@@ -214,8 +224,9 @@ __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
 // lane adds them).  No per-position bitmap, ranks or lane-to-lane hand-over:
 // the instruction count per tile follows the longest row, not the number of
 // lane boundaries the rows cross.
-template <typename T, bool STANDARD, bool UNIT, bool V32>
+template <typename T, bool STANDARD, bool UNIT, bool V32, int RPL>
 __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
+                                           const int64_t* __restrict__ ptr,
                                            const int64_t* __restrict__ idx,
                                            const T* __restrict__ val, const T* __restrict__ x,
                                            int64_t incx, T* __restrict__ y, int64_t incy,
@@ -223,7 +234,8 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
                                            int64_t re) {
   constexpr int64_t kAlign = V32 ? (sizeof(T) == 8 ? 4 : 8) : (sizeof(T) == 8 ? 2 : 4);
   const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
-  const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
+  const int64_t span =
+      (nr <= 32 ? __shfl_sync(0xffffffffu, re, nr - 1) : __ldg(ptr + r0 + nr)) - base;
   const int64_t a0 = base / kAlign * kAlign;
   const int lo = static_cast<int>(base - a0);
   const int window = static_cast<int>(span < kItems - lo ? span : kItems - lo);
@@ -241,21 +253,34 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
   for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = p[k];
   __syncwarp();
 
-  const bool mine = lane < nr;
-  const bool carries = !ends_here && lane == nr - 1;  // the row that runs on
+  // lane l sums rows l, l + 32, ... (tiles of more than 32 rows: the bounds of
+  // rows past the first 32 are read here)
+  const bool carries = !ends_here && lane == (nr - 1) % 32;  // owns the row that runs on
   T acc = T(0);
-  T* yp = mine ? &at<UNIT>(y, r0 + lane, incy) : nullptr;
-  if (mine) {
-    if (STANDARD) acc = *yp;
-    const int s0 = static_cast<int>(rb - a0);
-    const int e0 = static_cast<int>(re - a0 < lim ? re - a0 : lim);
+  T* yp = nullptr;
+#pragma unroll
+  for (int m = 0; m < RPL; ++m) {
+    if (32 * m >= nr) break;
+    const int k = lane + 32 * m;
+    if (k >= nr) continue;
+    const int64_t b = m == 0 ? rb : __ldg(ptr + r0 + k);
+    const int64_t e = m == 0 ? re : __ldg(ptr + r0 + k + 1);
+    T* rp = &at<UNIT>(y, r0 + k, incy);
+    T racc = STANDARD ? *rp : T(0);
+    const int s0 = static_cast<int>(b - a0);
+    const int e0 = static_cast<int>(e - a0 < lim ? e - a0 : lim);
     int q = s0;
     for (; q + 4 <= e0; q += 4) {
       const T u0 = w.prod[q], u1 = w.prod[q + 1], u2 = w.prod[q + 2], u3 = w.prod[q + 3];
-      acc = add_rn(add_rn(add_rn(add_rn(acc, u0), u1), u2), u3);
+      racc = add_rn(add_rn(add_rn(add_rn(racc, u0), u1), u2), u3);
     }
-    for (; q < e0; ++q) acc = add_rn(acc, w.prod[q]);
-    if (!carries) *yp = finish<true, STANDARD>(acc, alpha, beta, yp);
+    for (; q < e0; ++q) racc = add_rn(racc, w.prod[q]);
+    if (carries && k == nr - 1) {
+      acc = racc;
+      yp = rp;
+    } else {
+      *rp = finish<true, STANDARD>(racc, alpha, beta, rp);
+    }
   }
   if (!ends_here) {
     // the last row past the window: rounds of 256 products, added in stored
@@ -288,15 +313,17 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
 // One tile: rows r0 .. r0 + nr - 1 (nr >= 1), whose ptr entries lane k holds
 // as rb = ptr[r0 + k], re = ptr[r0 + k + 1] (k < nr).  Shared by the
 // single-matrix and the batched kernels.
-template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false>
-__device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t* __restrict__ idx,
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false,
+          int RPL = 1>
+__device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t* __restrict__ ptr,
+                                         const int64_t* __restrict__ idx,
                                          const T* __restrict__ val, const T* __restrict__ x,
                                          int64_t incx, T* __restrict__ y, int64_t incy, T alpha,
                                          T beta, int64_t r0, int nr, int64_t rb, int64_t re,
                                          const SplitBlock* split = nullptr) {
   if constexpr (EXACT) {
-    exact_tile<T, STANDARD, UNIT, V32>(w, lane, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
-                                       rb, re);
+    exact_tile<T, STANDARD, UNIT, V32, RPL>(w, lane, ptr, idx, val, x, incx, y, incy, alpha, beta,
+                                            r0, nr, rb, re);
     return;
   }
   const unsigned lt_mask = (1u << lane) - 1u;
@@ -306,33 +333,40 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
   constexpr int64_t kAlign = V32 ? (sizeof(T) == 8 ? 4 : 8) : (sizeof(T) == 8 ? 2 : 4);
 
   const int64_t base = __shfl_sync(0xffffffffu, rb, 0);
-  const int64_t span = __shfl_sync(0xffffffffu, re, nr - 1) - base;
+  const int64_t span =
+      (nr <= 32 ? __shfl_sync(0xffffffffu, re, nr - 1) : __ldg(ptr + r0 + nr)) - base;
   const int64_t a0 = base / kAlign * kAlign;
   const int lo = static_cast<int>(base - a0);
   const int window = static_cast<int>(span < kItems - lo ? span : kItems - lo);
   const int lim = lo + window;
   const bool ends_here = span <= window;  // the last row ends in the window
 
-  // row-start bitmap (+ end marker at lim) and nonempty-row table
+  // row-start bitmap (+ end marker at lim) and nonempty-row table; lane l
+  // handles rows l, l + 32, ... (bounds past the first 32 rows read here)
   if (lane <= kItems / 32) w.bits[lane] = 0u;
   __syncwarp();
-  const bool mine = lane < nr;
-  const bool nonempty = mine && re > rb;
-  if (nonempty) {
-    const int s = static_cast<int>(rb - a0);
-    atomicOr(&w.bits[s >> 5], 1u << (s & 31));
+  int ne_before = 0;  // nonempty rows in earlier passes
+#pragma unroll
+  for (int m = 0; m < RPL; ++m) {
+    if (32 * m >= nr) break;
+    const int k = lane + 32 * m;
+    const bool mine = k < nr;
+    const int64_t b = m == 0 ? rb : (mine ? __ldg(ptr + r0 + k) : 0);
+    const int64_t e = m == 0 ? re : (mine ? __ldg(ptr + r0 + k + 1) : 0);
+    const bool nonempty = mine && e > b;
+    if (nonempty) {
+      const int sp = static_cast<int>(b - a0);
+      atomicOr(&w.bits[sp >> 5], 1u << (sp & 31));
+    }
+    const unsigned ne_mask = __ballot_sync(0xffffffffu, nonempty);
+    if (nonempty) w.rowid[ne_before + __popc(ne_mask & lt_mask)] = static_cast<int16_t>(k);
+    if (mine && !nonempty && !STANDARD) {  // empty row: y = alpha*(+0) + beta*y
+      T* yp = &at<UNIT>(y, r0 + k, incy);
+      *yp = finish<EXACT, STANDARD>(T(0), alpha, beta, yp);
+    }
+    ne_before += __popc(ne_mask);
   }
   if (lane == 0 && ends_here) atomicOr(&w.bits[lim >> 5], 1u << (lim & 31));
-  const unsigned ne_mask = __ballot_sync(0xffffffffu, nonempty);
-  if (nonempty) {
-    const int k = __popc(ne_mask & lt_mask);
-    w.rowid[k] = lane;
-    if (EXACT && STANDARD) w.yinit[k] = at<UNIT>(y, r0 + lane, incy);
-  }
-  if (mine && !nonempty && !STANDARD) {  // empty row: y = alpha*(+0) + beta*y
-    T* yp = &at<UNIT>(y, r0 + lane, incy);
-    *yp = finish<EXACT, STANDARD>(T(0), alpha, beta, yp);
-  }
   __syncwarp();
 
   // lane's 8 contiguous positions [8*lane, 8*lane + 8) of the window
@@ -381,7 +415,7 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
       }
       first_seg = false;
       ++rank;
-      acc = add<EXACT>(row_init<EXACT, STANDARD>(w.yinit[rank - 1]), p[i]);
+      acc = p[i];
     } else if (!(EXACT && first_seg)) {
       acc = add<EXACT>(acc, p[i]);
     }
@@ -513,7 +547,8 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
   __syncwarp();  // bitmap and row tables are rewritten by the next tile
 }
 
-template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false,
+          int RPL = 1>
 __global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
 seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
            const T* __restrict__ val, const T* __restrict__ x, int64_t incx, T* __restrict__ y,
@@ -540,7 +575,7 @@ seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
         int64_t b = rows;
         if (v < ntiles) {
           b = tile_row != nullptr ? __ldg(tile_row + v)
-                                  : first_row_at(ptr, rows, kRowWeight, v * kItems);
+                                  : first_row_at(ptr, rows, kRowWeight / RPL, v * kItems);
         }
         w.bnd[i] = b;
       }
@@ -568,8 +603,8 @@ seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
       re_n = lane < nr_n ? __ldg(ptr + r0_n + lane + 1) : 0;
     }
     if (nr == 0) continue;
-    seg_tile<T, EXACT, STANDARD, UNIT, SPLIT, V32>(w, lane, idx, val, x, incx, y, incy, alpha,
-                                                  beta, r0, nr, rb, re, &split);
+    seg_tile<T, EXACT, STANDARD, UNIT, SPLIT, V32, RPL>(w, lane, ptr, idx, val, x, incx, y, incy,
+                                                       alpha, beta, r0, nr, rb, re, &split);
   }
   (void)nnz;
 }
@@ -727,7 +762,7 @@ seg_batch_kernel(const ascb_batch_item* __restrict__ items, int64_t count,
       if (nr == 0) continue;
       const int64_t rb = lane < nr ? __ldg(ptr + r0 + lane) : 0;
       const int64_t re = lane < nr ? __ldg(ptr + r0 + lane + 1) : 0;
-      seg_tile<T, EXACT, false, UNIT>(w, lane, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
+      seg_tile<T, EXACT, false, UNIT>(w, lane, ptr, idx, val, x, incx, y, incy, alpha, beta, r0, nr,
                                       rb, re);
     }
   }
@@ -757,14 +792,14 @@ inline bool aligned32(const ascb_csr* a) {
   return ((reinterpret_cast<uintptr_t>(a->idx) | reinterpret_cast<uintptr_t>(a->val)) & 31u) == 0;
 }
 
-template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool V32>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool V32, int RPL>
 int launch_v(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
              const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count) {
-  auto kernel = seg_kernel<T, EXACT, STANDARD, UNIT, false, V32>;
+  auto kernel = seg_kernel<T, EXACT, STANDARD, UNIT, false, V32, RPL>;
   const int64_t warps_needed = (ntiles + 3) / 4;
   const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
   const int64_t resident_ctas = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) *
-                                resident<T, EXACT, STANDARD, UNIT, V32 ? 4 : 0>(kernel);
+                                resident<T, EXACT, STANDARD, UNIT, (V32 ? 4 : 0) + 16 * RPL>(kernel);
   const unsigned blocks = static_cast<unsigned>(
       ctas_needed < 1 ? 1 : (ctas_needed < resident_ctas ? ctas_needed : resident_ctas));
   kernel<<<blocks, kThreads, 0, stream>>>(
@@ -774,24 +809,24 @@ int launch_v(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb
   return static_cast<int>(cudaGetLastError());
 }
 
-template <typename T, bool EXACT, bool STANDARD, bool UNIT>
+template <typename T, bool EXACT, bool STANDARD, bool UNIT, int RPL>
 int launch(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
            const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count) {
   return aligned32(a)
-             ? launch_v<T, EXACT, STANDARD, UNIT, true>(stream, a, alpha, beta, x, y, tile_row,
-                                                       ntiles, sm_count)
-             : launch_v<T, EXACT, STANDARD, UNIT, false>(stream, a, alpha, beta, x, y, tile_row,
-                                                        ntiles, sm_count);
+             ? launch_v<T, EXACT, STANDARD, UNIT, true, RPL>(stream, a, alpha, beta, x, y,
+                                                            tile_row, ntiles, sm_count)
+             : launch_v<T, EXACT, STANDARD, UNIT, false, RPL>(stream, a, alpha, beta, x, y,
+                                                             tile_row, ntiles, sm_count);
 }
 
-template <typename T, bool STANDARD, bool UNIT, bool V32>
+template <typename T, bool STANDARD, bool UNIT, bool V32, int RPL>
 int launch_split_v(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
                    const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count,
                    const SplitBlock& split) {
-  auto kernel = seg_kernel<T, false, STANDARD, UNIT, true, V32>;
+  auto kernel = seg_kernel<T, false, STANDARD, UNIT, true, V32, RPL>;
   const int64_t warps_needed = (ntiles + 3) / 4;
   const int64_t ctas_needed = (warps_needed + kWarpsPerCta - 1) / kWarpsPerCta;
-  const int per_sm = resident<T, false, STANDARD, UNIT, V32 ? 5 : 2>(kernel);
+  const int per_sm = resident<T, false, STANDARD, UNIT, (V32 ? 5 : 2) + 16 * RPL>(kernel);
   const int64_t resident_ctas = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * per_sm;
   const unsigned blocks = static_cast<unsigned>(
       ctas_needed < 1 ? 1 : (ctas_needed < resident_ctas ? ctas_needed : resident_ctas));
@@ -808,27 +843,45 @@ int launch_split_v(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, cons
   return static_cast<int>(cudaGetLastError());
 }
 
-template <typename T, bool STANDARD, bool UNIT>
+template <typename T, bool STANDARD, bool UNIT, int RPL>
 int launch_split(cudaStream_t stream, const ascb_csr* a, T alpha, T beta, const ascb_vec* x,
                  const ascb_vec* y, const int64_t* tile_row, int64_t ntiles, int sm_count,
                  const SplitBlock& split) {
-  return aligned32(a) ? launch_split_v<T, STANDARD, UNIT, true>(stream, a, alpha, beta, x, y,
-                                                                tile_row, ntiles, sm_count, split)
-                      : launch_split_v<T, STANDARD, UNIT, false>(stream, a, alpha, beta, x, y,
-                                                                 tile_row, ntiles, sm_count, split);
+  return aligned32(a)
+             ? launch_split_v<T, STANDARD, UNIT, true, RPL>(stream, a, alpha, beta, x, y, tile_row,
+                                                           ntiles, sm_count, split)
+             : launch_split_v<T, STANDARD, UNIT, false, RPL>(stream, a, alpha, beta, x, y,
+                                                            tile_row, ntiles, sm_count, split);
 }
 
-template <typename T, bool EXACT>
+template <typename T, bool EXACT, int RPL>
 int by_form(cudaStream_t s, int form, const ascb_csr* a, double alpha, double beta,
             const ascb_vec* x, const ascb_vec* y, const int64_t* tiles, int64_t n, int sm) {
   const bool unit = x->stride == 1 && y->stride == 1;
   const T al = static_cast<T>(alpha), be = static_cast<T>(beta);
   if (form == ASCB_STANDARD) {
-    return unit ? launch<T, EXACT, true, true>(s, a, al, be, x, y, tiles, n, sm)
-                : launch<T, EXACT, true, false>(s, a, al, be, x, y, tiles, n, sm);
+    return unit ? launch<T, EXACT, true, true, RPL>(s, a, al, be, x, y, tiles, n, sm)
+                : launch<T, EXACT, true, false, RPL>(s, a, al, be, x, y, tiles, n, sm);
   }
-  return unit ? launch<T, EXACT, false, true>(s, a, al, be, x, y, tiles, n, sm)
-              : launch<T, EXACT, false, false>(s, a, al, be, x, y, tiles, n, sm);
+  return unit ? launch<T, EXACT, false, true, RPL>(s, a, al, be, x, y, tiles, n, sm)
+              : launch<T, EXACT, false, false, RPL>(s, a, al, be, x, y, tiles, n, sm);
+}
+
+template <int RPL>
+int seg_rows(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
+             double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
+             int64_t ntiles, int sm_count) {
+  auto s = static_cast<cudaStream_t>(stream);
+  if (dtype == ASCB_F64) {
+    return exact ? by_form<double, true, RPL>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                              sm_count)
+                 : by_form<double, false, RPL>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                               sm_count);
+  }
+  return exact ? by_form<float, true, RPL>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                           sm_count)
+               : by_form<float, false, RPL>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                            sm_count);
 }
 
 }  // namespace
@@ -838,13 +891,26 @@ extern "C" int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const
                              double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
                              const int64_t* tile_row, int64_t ntiles, int sm_count) {
   if (ntiles <= 0) return 0;
-  auto s = static_cast<cudaStream_t>(stream);
-  if (dtype == ASCB_F64) {
-    return exact ? ascb::by_form<double, true>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count)
-                 : ascb::by_form<double, false>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count);
+  return ascb::seg_rows<1>(stream, dtype, form, exact, a, alpha, beta, x, y, tile_row, ntiles,
+                           sm_count);
+}
+
+extern "C" int64_t ascb_seg_tile_row_weight(void) { return ascb::kSegWeight; }
+
+extern "C" int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, const ascb_csr* a,
+                               double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
+                               const int64_t* tile_row, int64_t ntiles, int64_t weight,
+                               int sm_count) {
+  if (ntiles <= 0) return 0;
+  if (weight == ascb::kRowWeight) {
+    return ascb::seg_rows<1>(stream, dtype, form, exact, a, alpha, beta, x, y, tile_row, ntiles,
+                             sm_count);
   }
-  return exact ? ascb::by_form<float, true>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count)
-               : ascb::by_form<float, false>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count);
+  if (weight == ascb::kSegWeight) {
+    return ascb::seg_rows<ascb::kMaxRowsPerLane>(stream, dtype, form, exact, a, alpha, beta, x, y,
+                                                 tile_row, ntiles, sm_count);
+  }
+  return static_cast<int>(cudaErrorInvalidValue);
 }
 
 extern "C" int ascb_spmv_seg_alignment(void) { return 16; }
@@ -873,18 +939,18 @@ SplitLayout split_layout(int64_t nnz, int64_t split_min) {
   return l;
 }
 
-template <typename T>
+template <typename T, int RPL>
 int split_typed(cudaStream_t s, int form, const ascb_csr* a, double alpha, double beta,
                 const ascb_vec* x, const ascb_vec* y, const int64_t* tiles, int64_t n, int sm,
                 const SplitBlock& b) {
   const bool unit = x->stride == 1 && y->stride == 1;
   const T al = static_cast<T>(alpha), be = static_cast<T>(beta);
   if (form == ASCB_STANDARD) {
-    return unit ? launch_split<T, true, true>(s, a, al, be, x, y, tiles, n, sm, b)
-                : launch_split<T, true, false>(s, a, al, be, x, y, tiles, n, sm, b);
+    return unit ? launch_split<T, true, true, RPL>(s, a, al, be, x, y, tiles, n, sm, b)
+                : launch_split<T, true, false, RPL>(s, a, al, be, x, y, tiles, n, sm, b);
   }
-  return unit ? launch_split<T, false, true>(s, a, al, be, x, y, tiles, n, sm, b)
-              : launch_split<T, false, false>(s, a, al, be, x, y, tiles, n, sm, b);
+  return unit ? launch_split<T, false, true, RPL>(s, a, al, be, x, y, tiles, n, sm, b)
+              : launch_split<T, false, false, RPL>(s, a, al, be, x, y, tiles, n, sm, b);
 }
 
 }  // namespace
@@ -897,9 +963,12 @@ extern "C" size_t ascb_split_bytes(int64_t nnz, int64_t split_min) {
 
 extern "C" int ascb_spmv_split(void* stream, int dtype, int form, const ascb_csr* a, double alpha,
                                double beta, const ascb_vec* x, const ascb_vec* y,
-                               const int64_t* tile_row, int64_t ntiles, int64_t split_min,
-                               void* block, int sm_count) {
+                               const int64_t* tile_row, int64_t ntiles, int64_t weight,
+                               int64_t split_min, void* block, int sm_count) {
   if (ntiles <= 0) return 0;
+  if (weight != ascb::kRowWeight && weight != ascb::kSegWeight) {
+    return static_cast<int>(cudaErrorInvalidValue);
+  }
   if (split_min < ascb::kItems) split_min = ascb::kItems;
   const ascb::SplitLayout l = ascb::split_layout(a->nnz, split_min);
   auto* base = static_cast<unsigned char*>(block);
@@ -915,10 +984,18 @@ extern "C" int ascb_spmv_split(void* stream, int dtype, int form, const ascb_csr
   b.max_entries = l.entries;
   b.max_chunks = l.chunks;
   b.split_min = split_min;
-  if (dtype == ASCB_F64) {
-    return ascb::split_typed<double>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count, b);
+  constexpr int kR = ascb::kMaxRowsPerLane;
+  if (weight == ascb::kSegWeight && kR > 1) {
+    return dtype == ASCB_F64
+               ? ascb::split_typed<double, kR>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                               sm_count, b)
+               : ascb::split_typed<float, kR>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                              sm_count, b);
   }
-  return ascb::split_typed<float>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count, b);
+  return dtype == ASCB_F64 ? ascb::split_typed<double, 1>(s, form, a, alpha, beta, x, y, tile_row,
+                                                          ntiles, sm_count, b)
+                           : ascb::split_typed<float, 1>(s, form, a, alpha, beta, x, y, tile_row,
+                                                         ntiles, sm_count, b);
 }
 
 namespace ascb {

@@ -243,9 +243,11 @@ ASC_SB_API int asc_sb_csr_spmv(asc_sb_context* context, double alpha,
  * which forbids raw device allocations by plugins, and latency-critical loops
  * that must not risk the implicit device synchronisation of cudaMalloc or
  * cudaFree.  Same validation, error codes and arithmetic as asc_sb_csr_spmv
- * with the context's determinism; it always runs the default kernel and
- * ignores a variant forced with asc_sb_context_set_variant, so its results
- * equal asc_sb_csr_spmv's when the context's variant is AUTO.  Its only
+ * with the context's determinism; it always runs the default kernel,
+ * ignoring a variant forced with asc_sb_context_set_variant or picked by the
+ * selector.  In DETERMINISTIC mode its results equal asc_sb_csr_spmv's bit
+ * for bit; in BACKEND_DEFAULT mode both meet the same error bound and are
+ * equal whenever asc_sb_csr_spmv also runs the default kernel.  Its only
  * scratch, the row-tile partition, is a static 2 MiB device array per GPU
  * (held from library load until process exit): matrices needing more than
  * 262,144 tile bounds -- ceil((8*rows + nnz)/256) + 1 -- are rejected with
@@ -266,8 +268,11 @@ ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, double alpha,
  * (blas.h:1607-1667).  alpha_imag must be 0 (real element kinds).  CSR and
  * CSC are both accepted: CSC with op = none is computed as the transpose of
  * the CSR matrix with the same arrays.  A transpose (of CSR) in
- * DETERMINISTIC mode needs the transposed structure, which lives in a plan
- * (asc_sb_plan_create); without one the call returns ASC_SB_INVALID_STATE. */
+ * DETERMINISTIC mode runs on the transposed structure: a plan's
+ * (asc_sb_plan_create with ASC_SB_PLAN_TRANSPOSE), or, without a plan, one
+ * rebuilt for the call in the context's scratch buffer (which grows, after a
+ * stream drain, from the context's allocator).  BACKEND_DEFAULT without a
+ * plan scatters with atomics. */
 ASC_SB_API int asc_sb_standard_spmv(asc_sb_context* context, int32_t op,
                                     double alpha_real, double alpha_imag,
                                     const asc_sb_sparse* matrix,

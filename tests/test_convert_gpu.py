@@ -151,14 +151,14 @@ def test_deterministic_transposed_spmv_through_plan(cuda_lib, restatement, dt):
     y0 = rng.uniform(-1, 1, a_h.cols).astype(dt)
     ctx = context()
     a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
-    with pytest.raises(AscError) as e:
-        CudaSpmv(ctx, SparseBlasTranspose.kTranspose, 1.0, a, vec(dev(x_h), writable=False),
-                 vec(dev(y0)))
-    assert e.value.code == ErrorCode.kInvalidState
-    plan = CsrPlan(ctx, a, PLAN_TRANSPOSE)
     expect = y0.copy()
     restatement.standard_spmv(CSR, OP_TRANSPOSE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val,
                               -0.75, x_h, expect)
+    # without a plan: the transposed structure is rebuilt in the context's scratch
+    y = dev(y0)
+    CudaSpmv(ctx, SparseBlasTranspose.kTranspose, -0.75, a, vec(dev(x_h), writable=False), vec(y))
+    assert bits_equal(host(y), expect)
+    plan = CsrPlan(ctx, a, PLAN_TRANSPOSE)
     for op in (SparseBlasTranspose.kTranspose, SparseBlasTranspose.kConjugateTranspose):
         y = dev(y0)
         CudaSpmv(ctx, op, -0.75, a, vec(dev(x_h), writable=False), vec(y), plan=plan)

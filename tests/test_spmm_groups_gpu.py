@@ -3,7 +3,7 @@ DETERMINISTIC products equal the oracle bit for bit -- every row still adds
 its entries in stored order -- for every group size the autotuner can pick,
 ragged shapes (empty rows, long rows, a last group shorter than R), FP32 and
 FP64 and several k; BACKEND_DEFAULT stays within
-|c - c_ref| <= gamma_{n+2} |alpha| sum|a b| + gamma_2 |c0| of the long-double
+|c - c_ref| <= gamma_{n+2} (|alpha| sum|a b| + |c0|) of the long-double
 oracle."""
 
 import numpy as np
@@ -84,7 +84,7 @@ def test_row_groups_default_mode_within_bound(cuda_lib, restatement, dt):
                                                  a_h.val, bj)
             ref = c0[:, j].astype(np.longdouble) + 0.75 * exact
             rep = oracle.error_report(got[:, j], ref, absval, counts, dt, 0.75,
-                                      2 * np.finfo(dt).eps * np.abs(c0[:, j].astype(np.float64)))
+                                      np.abs(c0[:, j].astype(np.float64)))
             assert rep["max_ratio_to_bound"] <= 1.0, (name, j, rep)
         plan.close()
     ctx.close()
