@@ -226,6 +226,80 @@ def headline_error(a, x, y_best, y_det, mode):
     return rep
 
 
+def spmv_error(a, x, got, transpose):
+    """y = A x (or A^T x) from y = 0, DETERMINISTIC and BACKEND_DEFAULT, against
+    the oracle: the C restatement in the data's precision for bit-exactness,
+    its long-double sums for the bound gamma_{n+2} sum|a x| per output."""
+    import oracle as orc
+    rs = orc.Restatement()
+    op = orc.OP_TRANSPOSE if transpose else orc.OP_NONE
+    want = np.zeros(a.cols if transpose else a.rows, dtype=a.val.dtype)
+    rs.standard_spmv(orc.CSR, op, a.rows, a.cols, a.ptr, a.idx, a.val, 1.0, x, want)
+    exact, absval = rs.extended(op, a.rows, a.cols, a.ptr, a.idx, a.val, x)
+    counts = np.bincount(a.idx, minlength=a.cols) if transpose else np.diff(a.ptr)
+    rep = orc.error_report(got["default"], exact, absval, counts, a.val.dtype, 1.0)
+    rep.update({"mode": "backend_default (plan)",
+                "deterministic_bitexact": bool(got["deterministic"].tobytes() == want.tobytes()),
+                "bound": "|y - y_ref| <= gamma_{n+2} sum|a x| per output",
+                "oracle": "C restatement of asc::Spmv (blas.h:1607-1667), long double for the bound"})
+    return rep
+
+
+def batch_error(g, got, sample):
+    """y = A_m x_m for `sample` matrices spread over the batch, both modes,
+    against the oracle's compat form (the C restatement of
+    CudaCsrSpmv's y = alpha A x + beta y in FP64): DETERMINISTIC bit for bit,
+    BACKEND_DEFAULT within gamma_{n+2} sum|a x| per row."""
+    import oracle as orc
+    rs = orc.Restatement()
+    ptr, idx, val, x = (g[k].cpu().numpy() for k in ("ptr", "idx", "val", "x"))
+    count = len(g["rows"])
+    worst, exact_all, outputs = 0.0, True, 0
+    for m in np.linspace(0, count - 1, min(sample, count)).astype(np.int64):
+        n, z = int(g["rows"][m]), int(g["nnz"][m])
+        pb, nb, rb = int(g["ptr_base"][m]), int(g["nz_base"][m]), int(g["row_base"][m])
+        p, i, v, xm = ptr[pb:pb + n + 1], idx[nb:nb + z], val[nb:nb + z], x[rb:rb + n]
+        want = rs.compat_spmv(p, i, v, 1.0, xm, 0.0, np.zeros(n))
+        exact_all &= got["deterministic"][rb:rb + n].tobytes() == want.tobytes()
+        e, a = rs.extended(orc.OP_NONE, n, n, p, i, v, xm)
+        rep = orc.error_report(got["default"][rb:rb + n], e, a, np.diff(p), np.float64, 1.0)
+        worst = max(worst, rep["max_ratio_to_bound"])
+        outputs += n
+    return {"mode": "backend_default (batch kernel)", "max_ratio_to_bound": worst,
+            "deterministic_bitexact": bool(exact_all), "outputs": outputs,
+            "sample": f"{min(sample, count)} matrices spread over the batch",
+            "bound": "|y - y_ref| <= gamma_{n+2} sum|a x| per row",
+            "oracle": "C restatement of the compat SpMV (FP64), long double for the bound"}
+
+
+def spmm_error(a, b, c, mode, sample_rows, tensor_cores=False):
+    """Error of an SpMM result C = A B (FP32) against the FP64 oracle (the C
+    restatement run in FP64 on the same inputs) on the first `sample_rows`
+    rows, with the bound gamma_{n+2} sum|a b| (+ the FP64 oracle's own)."""
+    import oracle as orc
+    rs = orc.Restatement()
+    rows = min(a.rows, sample_rows)
+    ptr = a.ptr[:rows + 1]
+    nnz = int(ptr[-1])
+    idx, val = a.idx[:nnz], a.val[:nnz].astype(np.float64)
+    b64 = b.astype(np.float64)
+    ref = orc.standard_spmm_rows(rs, a.cols, ptr, idx, val, 1.0, b64, np.zeros((rows, b.shape[1])))
+    absval = orc.standard_spmm_rows(rs, a.cols, ptr, idx, np.abs(val), 1.0, np.abs(b64),
+                                    np.zeros((rows, b.shape[1])))
+    counts = np.diff(ptr)[:, None]
+    if tensor_cores:  # 3xTF32 on the tensor cores
+        bound = ((counts + 64) * 2.0 ** -22 + orc.gamma(counts + 2, np.float64)) * absval
+    else:
+        bound = (orc.gamma(counts + 2, np.float32) + orc.gamma(counts + 2, np.float64)) * absval
+    bound = bound + np.finfo(np.float32).tiny
+    err = np.abs(c[:rows].astype(np.float64) - ref)
+    return {"mode": mode, "max_abs": float(err.max()),
+            "max_ratio_to_bound": float((err / bound).max()),
+            "bound": "|c - c_ref| <= gamma_{n+2} sum|a b| per output (tensor-core 3xTF32: "
+                     "(n+64) 2^-22 sum|a b|)",
+            "sample": f"first {rows} rows", "oracle": "C restatement in FP64"}
+
+
 def cusparse_leg(a, A, x, stream, bytes_step):
     """cuSPARSE SpMV (torch's CSR mat-vec) on the same device arrays: a
     library comparison, timed like the headline; never the product."""
@@ -628,6 +702,17 @@ def run_extra(args):
             ctx.set_determinism(det)
             ms = timed(lambda: sc.CudaSpmv(ctx, op, 1.0, A, xv, yv, plan=plan if use_plan else None))
             detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1)}
+        # one product of each mode through the plan against the oracle (the
+        # checker; after every timed region): y = 0 + A x or A^T x
+        got = {}
+        for name, det in (("deterministic", Determinism.kDeterministic),
+                          ("default", Determinism.kBackendDefault)):
+            ctx.set_determinism(det)
+            y.zero_()
+            sc.CudaSpmv(ctx, op, 1.0, A, xv, yv, plan=plan)
+            stream.synchronize()
+            got[name] = y.cpu().numpy()
+        extra_cfg["error_vs_fp64_oracle"] = spmv_error(a_h, x.cpu().numpy(), got, transpose)
         plan.close()
         dtype_s = "f32" if dt == np.float32 else "f64"
         extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "op": "transpose" if transpose else "none"})
@@ -646,16 +731,44 @@ def run_extra(args):
         flops = 2 * a_h.nnz * k
         bv = sc.DenseMatrixView(B, a_h.cols, k, writable=False)
         cv = sc.DenseMatrixView(C, a_h.rows, k)
-        plan = sc.CsrPlan(ctx, A)  # detects dense 16 x 16 blocks (tensor-core path)
+        from asc_cpp_b200._abi import PLAN_HAS_ROW_GROUPS, PLAN_ROW_GROUPS
+        # a plan detects dense 16 x 16 blocks (tensor-core path) and builds the
+        # row groups (B rows shared by neighbouring rows)
+        plan = sc.CsrPlan(ctx, A, PLAN_ROW_GROUPS)
         extra_cfg["dense_blocks16"] = bool(plan.properties() & 2)
+        extra_cfg["row_groups_kept"] = bool(plan.properties() & PLAN_HAS_ROW_GROUPS)
+        plain = sc.CsrPlan(ctx, A)
         for name, det in (("deterministic", Determinism.kDeterministic),
                           ("default", Determinism.kBackendDefault)):
             ctx.set_determinism(det)
+            for tag, p_ in (("", plain), ("_row_groups", plan)):
+                ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv,
+                                               plan=p_))
+                detail[name + tag] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
+                                      "gflops": round(flops / ms / 1e6, 1)}
+            # the SpMM autotuner on this k (row by row, or R rows per group)
+            scratch = torch.zeros_like(C)
+            t_ms, rg = plan.spmm_autotune(1.0, bv, sc.DenseMatrixView(scratch, a_h.rows, k), 5)
             ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv,
                                            plan=plan))
-            detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
-                            "gflops": round(flops / ms / 1e6, 1)}
+            detail[name + "_autotuned"] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
+                                           "gflops": round(flops / ms / 1e6, 1),
+                                           "rows_per_group": rg}
+            del scratch
+        # the fastest default-mode product against the FP64 oracle on a row
+        # sample (the checker; after every timed region)
+        best_default = min((kk for kk in detail if kk.startswith("default")),
+                           key=lambda kk: detail[kk]["ms"])
+        ctx.set_determinism(Determinism.kBackendDefault)
+        use = plain if best_default == "default" else plan
+        C.zero_()
+        sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv, plan=use)
+        stream.synchronize()
+        extra_cfg["error_vs_fp64_oracle"] = spmm_error(a_h, B.cpu().numpy(), C.cpu().numpy(),
+                                                       best_default, 65_536,
+                                                       extra_cfg["dense_blocks16"])
         plan.close()
+        plain.close()
         dtype_s = "f32"
         extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "k": k, "layout": "row-major, ld=k"})
     elif w.startswith("sptrsv"):
@@ -711,6 +824,7 @@ def run_extra(args):
             ctx.set_determinism(det)
             ms = timed(lambda: solve(use_plan)) - copy_ms
             detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1)}
+        solved = {}
         t0 = time.perf_counter()
         plan.triangular_analysis(SparseBlasTranspose.kNone, SparseBlasTriangle.kLower)
         stream.synchronize()
@@ -720,6 +834,8 @@ def run_extra(args):
             ctx.set_determinism(det)
             ms = timed(lambda: solve(True)) - copy_ms
             detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1)}
+            stream.synchronize()
+            solved[name] = xb.cpu().numpy()  # x = A^-1 b0, the same every timed call
         plan.close()
         try:  # the library baseline: cuSPARSE SpSV through torch (not on the product path)
             At = torch.sparse_csr_tensor(A.offsets, A.indices, A.values, (n, n))
@@ -734,8 +850,19 @@ def run_extra(args):
         r = Restatement()
         bh = b0.cpu().numpy()
         t0 = time.perf_counter()
-        r.triangular_solve(0, 1, int(diag), n, a_h.ptr, a_h.idx, a_h.val, 1.0, bh)
+        want = r.triangular_solve(0, 1, int(diag), n, a_h.ptr, a_h.idx, a_h.val, 1.0, bh)
         detail["cpu_oracle_1_thread"] = {"ms": round((time.perf_counter() - t0) * 1e3, 2)}
+        # the level-scheduled solves against the oracle's row-by-row solve:
+        # DETERMINISTIC bit for bit; BACKEND_DEFAULT by its largest relative
+        # difference (a solve's error grows along dependency chains, so no
+        # per-row bound is claimed)
+        dd = solved["default_levels"].astype(np.float64) - want
+        extra_cfg["error_vs_fp64_oracle"] = {
+            "deterministic_bitexact": bool(solved["deterministic_levels"].tobytes() == want.tobytes()),
+            "default_max_abs": float(np.abs(dd).max()),
+            "default_max_rel": float((np.abs(dd) / np.maximum(np.abs(want), 1e-300)).max()),
+            "outputs": int(n),
+            "oracle": "C restatement of the row-by-row triangular solve, same precision"}
         dtype_s = "f32" if dt == np.float32 else "f64"
         extra_cfg.update({"rows": n, "nnz": a_h.nnz, "op": "none", "triangle": "lower",
                           "rhs_restore_ms_subtracted": round(copy_ms, 4)})
@@ -819,6 +946,7 @@ def run_extra(args):
             xs.append(sc.CudaStridedVectorView(g["x"][rb:rb + n], n, writable=False))
             ys.append(sc.CudaStridedVectorView(g["y"][rb:rb + n], n))
         batch = sc.CudaBatch(ctx, mats, xs, ys)
+        got = {}
         byts = int((g["nnz"] * 16 + (g["rows"] + 1) * 8 + 2 * g["rows"] * 8).sum())
         for name, det in (("deterministic", Determinism.kDeterministic),
                           ("default", Determinism.kBackendDefault)):
@@ -832,7 +960,10 @@ def run_extra(args):
             detail[name] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
                             "per_matrix_ms": round(per, 3), "speedup_vs_per_matrix": round(per / ms, 2),
                             "schedule": batch.schedule()}
+            stream.synchronize()
+            got[name] = g["y"].cpu().numpy()  # y = A x, the same every timed call
         batch.close()
+        extra_cfg["error_vs_fp64_oracle"] = batch_error(g, got, 128)
         dtype_s = "f64"
         extra_cfg.update({"matrices": 4096, "rows": int(g["rows"].sum()), "nnz": int(g["nnz"].sum())})
     if w.startswith("level1"):
