@@ -216,10 +216,15 @@ std::size_t WarpTileBytes(std::int64_t rows, std::int64_t nnz) {
   return RoundUp(static_cast<std::size_t>(WarpTiles(rows, nnz) + 1) * 8, 256);
 }
 std::int64_t SegTiles(std::int64_t rows, std::int64_t nnz) {
-  return ascb_row_tile_count(rows, nnz, ascb_warp_tile_items(), ascb_seg_tile_row_weight());
+  return ascb_row_tile_count(rows, nnz, ascb_seg_tile_items(), ascb_seg_tile_row_weight());
 }
 std::size_t SegTileBytes(std::int64_t rows, std::int64_t nnz) {
   return RoundUp(static_cast<std::size_t>(SegTiles(rows, nnz) + 1) * 8, 256);
+}
+// Room for either row-tile partition (the segmented kernel's has fewer tiles
+// unless rows average more than about 300 entries).
+std::size_t TileBytes(std::int64_t rows, std::int64_t nnz) {
+  return std::max(WarpTileBytes(rows, nnz), SegTileBytes(rows, nnz));
 }
 std::size_t MergeBoundBytes(std::int64_t rows, std::int64_t nnz) {
   return RoundUp(static_cast<std::size_t>(ascb_merge_tiles(rows, nnz) + 1) * 16, 256);
@@ -237,7 +242,7 @@ std::size_t SplitBlockBytes(std::int64_t nnz) {
 }
 std::size_t CompatWorkspaceBytes(const asc_sb_sparse& m) {
   if (m.rows == 0 || m.columns == 0) return 0;
-  return std::max(WarpTileBytes(m.rows, m.nonzeros) + SplitBlockBytes(m.nonzeros),
+  return std::max(TileBytes(m.rows, m.nonzeros) + SplitBlockBytes(m.nonzeros),
                   MergeBoundBytes(m.rows, m.nonzeros));
 }
 
@@ -324,13 +329,13 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
        static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
   const std::int64_t weight =
       seg_aligned ? ascb_seg_tile_row_weight() : ascb_warp_tile_row_weight();
-  const std::int64_t tiles = ascb_row_tile_count(a.rows, a.nnz, ascb_warp_tile_items(), weight);
+  const std::int64_t items = seg_aligned ? ascb_seg_tile_items() : ascb_warp_tile_items();
+  const std::int64_t tiles = ascb_row_tile_count(a.rows, a.nnz, items, weight);
   const std::int64_t* tiles_ptr =
       planned != nullptr ? (seg_aligned ? planned->seg_tiles : planned->warp_tiles) : nullptr;
   if (tiles_ptr == nullptr && scratch != nullptr) {
     Status s = Launched(ctx,
-                        ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(), weight, scratch,
-                                       tiles),
+                        ascb_row_tiles(ctx->stream, &a, items, weight, scratch, tiles),
                         "CUDA could not launch the row-tile partition kernel");
     if (!s.ok()) return s;
     tiles_ptr = scratch;
@@ -342,7 +347,7 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
     void* block = planned != nullptr ? planned->split
                   : scratch != nullptr
                       ? static_cast<void*>(reinterpret_cast<unsigned char*>(scratch) +
-                                           WarpTileBytes(a.rows, a.nnz))
+                                           TileBytes(a.rows, a.nnz))
                       : nullptr;
     if (block != nullptr) {
       const std::int64_t rounds = choice.lanes > 0 ? choice.lanes : kSplitRounds;
@@ -386,7 +391,7 @@ Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* bu
                       "CUDA could not launch the row-tile partition kernel");
   if (!s.ok()) return s;
   s = Launched(ctx,
-               ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(), ascb_seg_tile_row_weight(),
+               ascb_row_tiles(ctx->stream, &a, ascb_seg_tile_items(), ascb_seg_tile_row_weight(),
                               seg, out->n_seg),
                "CUDA could not launch the row-tile partition kernel");
   if (!s.ok()) return s;

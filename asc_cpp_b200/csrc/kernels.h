@@ -90,6 +90,10 @@ int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const ascb_csr* 
 // segmented kernel's own partition: more rows per tile, so more of each
 // window holds nonzeros when rows are short).
 int64_t ascb_seg_tile_row_weight(void);
+// Weighted items per tile of that partition (ascb_row_tiles' `items`): fewer
+// than ascb_warp_tile_items() when the weight is small, so that every row of
+// a tile but the first starts inside the tile's 256-position window.
+int64_t ascb_seg_tile_items(void);
 int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
                     double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
                     int64_t ntiles, int64_t weight, int sm_count);

@@ -12,10 +12,12 @@
 //
 // Limits and rules, stated for users:
 //   * the array holds kNoAllocMaxBounds int64 tile bounds (2 MiB per GPU); a
-//     matrix needs ceil((8*rows + nnz) / 256) + 1 of them, so up to about
-//     67 million weighted items (for example 4 million rows with 33 million
-//     nonzeros).  Larger matrices are rejected with ASC_SB_UNSUPPORTED and a
-//     message naming the limit;
+//     matrix whose index and value arrays start on 16-byte boundaries needs
+//     ceil((2*rows + nnz) / 251) + 1 of them (the segmented kernel's row
+//     tiles, as asc_sb_csr_spmv uses), so up to about 65 million weighted
+//     items (for example 4 million rows with 57 million nonzeros); other
+//     matrices need ceil((8*rows + nnz) / 256) + 1.  Larger matrices are
+//     rejected with ASC_SB_UNSUPPORTED and a message naming the limit;
 //   * every call on a device shares the one array.  Calls whose work overlaps
 //     on the GPU -- two streams, or two contexts on the same device, without
 //     ordering between them -- race on it and may compute wrong results;
@@ -130,8 +132,13 @@ extern "C" ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, doub
   }
   if (matrix->rows == 0) return Done(v, ASC_SB_OK, "");
 
-  const int64_t items = ascb_warp_tile_items();
-  const int64_t weight = ascb_warp_tile_row_weight();
+  // the partition asc_sb_csr_spmv uses for the same arrays
+  const bool seg_aligned =
+      ((reinterpret_cast<std::uintptr_t>(matrix->structure_second) |
+        reinterpret_cast<std::uintptr_t>(matrix->values)) &
+       static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
+  const int64_t items = seg_aligned ? ascb_seg_tile_items() : ascb_warp_tile_items();
+  const int64_t weight = seg_aligned ? ascb_seg_tile_row_weight() : ascb_warp_tile_row_weight();
   const int64_t tiles = ascb_row_tile_count(matrix->rows, matrix->nonzeros, items, weight);
   if (tiles + 1 > kNoAllocMaxBounds) {
     return Done(v, ASC_SB_UNSUPPORTED,
@@ -162,11 +169,8 @@ extern "C" ASC_SB_API int asc_sb_csr_spmv_no_alloc(asc_sb_context* context, doub
   int rc = ascb_row_tiles(v.stream, &a, items, weight, scratch, tiles);
   v.launches->fetch_add(1, std::memory_order_relaxed);
   if (rc == 0) {
-    const bool seg_aligned =
-        ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
-         static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
-    rc = seg_aligned ? ascb_spmv_seg(v.stream, dtype, ASCB_COMPAT, exact, &a, alpha, beta, &xv, &yv,
-                                   scratch, tiles, v.sm_count)
+    rc = seg_aligned ? ascb_spmv_seg_w(v.stream, dtype, ASCB_COMPAT, exact, &a, alpha, beta, &xv,
+                                       &yv, scratch, tiles, weight, v.sm_count)
                    : ascb_spmv_warp(v.stream, dtype, ASCB_COMPAT, exact, &a, alpha, beta, &xv, &yv,
                                     scratch, tiles, v.sm_count);
     v.launches->fetch_add(1, std::memory_order_relaxed);

@@ -42,6 +42,17 @@ constexpr int kMaxRowsPerLane = kRowWeight / kSegWeight;  // rows per lane in a 
 constexpr int kMaxRows = 32 * kMaxRowsPerLane;
 static_assert(kRowWeight % kSegWeight == 0 && kMaxRowsPerLane >= 1 && kMaxRowsPerLane <= 8,
               "the segmented kernel's row weight divides 8");
+// A window starts on the aligned position at or before its tile's first
+// nonzero, up to kMaxLead positions earlier (FP32 with 32-byte loads).  Every
+// row of a tile but the first must start inside the window, so a tile of row
+// weight W spans at most tile_items<RPL>() weighted items: its other rows then
+// start at most items - 1 - W <= kItems - 1 - kMaxLead positions past its
+// first row's start (the warp tiles' W = 8 needs no reduction).
+constexpr int kMaxLead = 7;
+template <int RPL>
+__host__ __device__ constexpr int64_t tile_items() {
+  return kRowWeight / RPL >= kMaxLead ? kItems : kItems - kMaxLead + kRowWeight / RPL;
+}
 constexpr int kPer = 8;            // contiguous positions per lane
 constexpr int kChunk = 32;         // tile bounds cached per warp
 constexpr int kMaxDevices = 64;
@@ -575,7 +586,7 @@ seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
         int64_t b = rows;
         if (v < ntiles) {
           b = tile_row != nullptr ? __ldg(tile_row + v)
-                                  : first_row_at(ptr, rows, kRowWeight / RPL, v * kItems);
+                                  : first_row_at(ptr, rows, kRowWeight / RPL, v * tile_items<RPL>());
         }
         w.bnd[i] = b;
       }
@@ -896,6 +907,9 @@ extern "C" int ascb_spmv_seg(void* stream, int dtype, int form, int exact, const
 }
 
 extern "C" int64_t ascb_seg_tile_row_weight(void) { return ascb::kSegWeight; }
+extern "C" int64_t ascb_seg_tile_items(void) {
+  return ascb::tile_items<ascb::kMaxRowsPerLane>();
+}
 
 extern "C" int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, const ascb_csr* a,
                                double alpha, double beta, const ascb_vec* x, const ascb_vec* y,

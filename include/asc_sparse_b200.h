@@ -250,8 +250,9 @@ ASC_SB_API int asc_sb_csr_spmv(asc_sb_context* context, double alpha,
  * equal whenever asc_sb_csr_spmv also runs the default kernel.  Its only
  * scratch, the row-tile partition, is a static 2 MiB device array per GPU
  * (held from library load until process exit): matrices needing more than
- * 262,144 tile bounds -- ceil((8*rows + nnz)/256) + 1 -- are rejected with
- * ASC_SB_UNSUPPORTED.  All calls on a device share that array: calls that
+ * 262,144 tile bounds -- ceil((2*rows + nnz)/251) + 1 when the index and
+ * value arrays start on 16-byte boundaries, ceil((8*rows + nnz)/256) + 1
+ * otherwise -- are rejected with ASC_SB_UNSUPPORTED.  All calls on a device share that array: calls that
  * overlap on the GPU race.  The first call on each device looks up the
  * array's device address, once; make that first call before any stream
  * capture starts on the device.  A cudaDeviceReset invalidates the address

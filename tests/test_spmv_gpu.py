@@ -325,7 +325,15 @@ def _shapes(rng, dt):
     ptr, idx = synthetic._unique_sorted_rows(rng, 30000, lengths)
     long_rows = synthetic.Csr(lengths.size, 30000, ptr, idx,
                               rng.standard_normal(int(ptr[-1])).astype(dt))
+    # rows of 0..8 and 240..255 entries: tiles whose window starts up to 7
+    # positions before their first row and whose second row starts ~250
+    # positions later (the edge of the 256-position window)
+    lead = np.where(rng.random(20000) < 0.5, rng.integers(0, 9, 20000),
+                    rng.integers(240, 256, 20000))
+    lptr, lidx = synthetic._unique_sorted_rows(rng, 30000, lead)
     return {
+        "window_leads": synthetic.Csr(lead.size, 30000, lptr, lidx,
+                                      rng.standard_normal(int(lptr[-1])).astype(dt)),
         "irregular": synthetic.random_csr(rng, 3000, 2500, 90, dt, 0.1),
         "long_rows": long_rows,
         "empty_rows": synthetic.random_csr(rng, 20000, 500, 6, dt, 0.9),

@@ -65,7 +65,9 @@ def test_no_alloc_rejects_matrices_beyond_its_scratch(cuda_lib):
     """A matrix whose partition does not fit the static scratch is refused with
     kUnsupported before anything runs; y is untouched."""
     ctx = context()
-    rows = 9_000_000  # needs 8*rows/256 + 1 = 281,251 tile bounds > 262,144
+    # needs ceil(2*rows/251) + 1 = 318,727 tile bounds (empty, so 16-byte
+    # aligned, index and value arrays) > 262,144
+    rows = 40_000_000
     ptr = torch.zeros(rows + 1, dtype=torch.int64, device="cuda")
     a = csr(2, 2, [0, 0, 0], np.zeros(0, np.int64), np.zeros(0))
     a.rows, a.columns, a.offsets = rows, 1, ptr
