@@ -85,6 +85,8 @@ PLAN_ROW_GROUPS = 4
 PLAN_HAS_TRANSPOSE = 1
 PLAN_HAS_BLOCKS16 = 2
 PLAN_HAS_ROW_GROUPS = 4
+PLAN_HAS_STAGED_SPMM = 8
+SPMM_STAGED = -1  # asc_sb_plan_spmm_autotune: the TMA-staged kernel won
 
 
 class SparseDesc(ctypes.Structure):
@@ -215,6 +217,9 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_spmm_autotune": (ctypes.c_int, [_P, _P, _D, _DP, _DP, _I32,
                                                  ctypes.POINTER(ctypes.c_float),
                                                  ctypes.POINTER(_I32)]),
+    "asc_sb_plan_spmm_tuning": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_I32),
+                                               ctypes.POINTER(_I32),
+                                               ctypes.POINTER(ctypes.c_float)]),
     "asc_sb_standard_triangular_solve": (ctypes.c_int, [_P, _I32, _D, _D, _SP, _I32, _I32,
                                                         _DP]),
     "asc_sb_plan_triangular_solve": (ctypes.c_int, [_P, _P, _I32, _D, _D, _I32, _I32, _DP]),

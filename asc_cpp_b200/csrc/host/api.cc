@@ -120,6 +120,18 @@ struct asc_sb_plan {
   ascb_row_groups groups{};
   std::int64_t group_run_count = 0;
   bool use_groups = false;  // SpMM through the groups (reuse measured or tuned)
+  // ASC_SB_PLAN_ROW_GROUPS also builds the TMA-staged SpMM tables (groups of
+  // 16 rows); caps[2w], caps[2w + 1]: largest slot and entry counts of a
+  // stage of 2^w groups
+  unsigned char* staged_mem = nullptr;
+  ascb_staged_spmm staged{};
+  std::int64_t staged_caps[10] = {};
+  bool has_staged = false;
+  bool use_staged = false;  // SpMM through the staged kernel where it fits
+  // the last SpMM autotune: candidates timed and their ms per product
+  int tuned_count = 0;
+  int tuned_candidate[8] = {};
+  float tuned_ms[8] = {};
 };
 
 namespace {
@@ -415,7 +427,7 @@ std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {
 struct PlanLayout {
   std::size_t flag = 0;  // one device int for structure checks
   std::size_t t_ptr = 0, t_idx = 0, t_perm = 0, t_val = 0, t_part = 0;
-  std::size_t sort = 0, outer_of = 0, solve = 0, analysis = 0, groups = 0, total = 0;
+  std::size_t sort = 0, outer_of = 0, solve = 0, analysis = 0, groups = 0, staged = 0, total = 0;
 };
 
 PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
@@ -457,6 +469,8 @@ PlanLayout PlanLayoutFor(const asc_sb_sparse& m, int flags) {
                       outer, nnz, static_cast<int>(ascb::host::ElementBytes(m.element_kind)))
                       .total,
                   256);
+    l.staged = at;
+    at += RoundUp(ascb_staged_layout_for(outer, nnz).total, 256);
   }
   l.total = at;
   return l;
@@ -486,6 +500,34 @@ Status BuildRowGroups(asc_sb_context* ctx, asc_sb_plan* plan, int rows_per_group
   }
   plan->group_run_count = runs;
   plan->use_groups = runs > 0 && 4 * a.nnz >= 5 * runs;
+  return Status::Ok();
+}
+
+// The TMA-staged SpMM tables, from row groups of 16 rows built just before
+// (their build scratch is read); reads back the stage caps (synchronizes the
+// stream).  Used by default when the groups share columns (at least 1.25
+// stored entries per distinct column of a group).
+Status BuildStaged(asc_sb_context* ctx, asc_sb_plan* plan) {
+  const ascb_csr a = AsCsr(plan->matrix, false);
+  const int elem = static_cast<int>(ascb::host::ElementBytes(plan->matrix.element_kind));
+  Status s = Launched(ctx,
+                      ascb_staged_build(ctx->stream, &a, &plan->groups, plan->groups_mem, elem,
+                                        plan->staged_mem, &plan->staged, ctx->sm_count),
+                      "CUDA could not launch the staged SpMM build");
+  if (!s.ok()) return s;
+  unsigned long long caps[10] = {};
+  cudaError_t e = cudaMemcpyAsync(caps, plan->staged.caps, sizeof(caps), cudaMemcpyDeviceToHost,
+                                  ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) {
+    (void)cudaGetLastError();
+    return {ASC_SB_PROVIDER, std::string("CUDA could not build the staged SpMM tables: ") +
+                                 cudaGetErrorString(e)};
+  }
+  for (int i = 0; i < 10; ++i) plan->staged_caps[i] = static_cast<std::int64_t>(caps[i]);
+  plan->has_staged = true;
+  const std::int64_t slots = plan->group_run_count;  // of the 16-row groups
+  plan->use_staged = slots > 0 && 4 * a.nnz >= 5 * slots;
   return Status::Ok();
 }
 
@@ -1125,6 +1167,32 @@ bool GroupsApply(const asc_sb_dense& b, const asc_sb_dense& c, int kind) {
           15u) == 0;
 }
 
+// The staged kernel's operand rules (those of the row groups) and the room
+// it needs: two stages of the plan's largest stage for this k in one CTA's
+// shared memory.  *ng, *slots, *entries: the stage width and its caps.
+bool StagedApply(const asc_sb_plan& plan, const asc_sb_dense& b, const asc_sb_dense& c, int kind,
+                 int device, std::int64_t* slots, std::int64_t* entries) {
+  if (!plan.has_staged || !GroupsApply(b, c, kind)) return false;
+  const int dtype = Dtype(kind);
+  // at most 128 chunks of 16 bytes per row (32 lanes x 4 chunks)
+  if (c.columns * static_cast<std::int64_t>(ascb::host::ElementBytes(kind)) > 128 * 16) {
+    return false;
+  }
+  const int ng = ascb_staged_groups_per_stage(dtype, c.columns);
+  int w = 0;
+  while ((1 << w) < ng) ++w;
+  *slots = plan.staged_caps[2 * w];
+  *entries = plan.staged_caps[2 * w + 1];
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) !=
+      cudaSuccess) {
+    (void)cudaGetLastError();
+    return false;
+  }
+  const std::size_t stage = ascb_staged_stage_bytes(dtype, c.columns, *slots, *entries, ng);
+  return 2 * stage <= static_cast<std::size_t>(optin);
+}
+
 // C += alpha * op(A) * B, validated in full before anything is enqueued.  With
 // a plan that holds the transposed structure, a transposed product runs the
 // stored-order kernel on that structure (bit-exact); without one it scatters.
@@ -1178,13 +1246,18 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
     // dense 16 x 16 blocks: tensor cores (3xTF32), within the bound stated in
     // spmm_block16_tc.cu; faster than the CUDA-core kernels at every k
     // measured on B200 (65,536-row 2% block-sparse matrix, k = 8 / 32 / 128:
-    // 0.48 / 0.51 / 0.62 ms against 0.80 / 1.05 / 2.04 ms)
+    // 0.48 / 0.51 / 0.62 ms against 0.80 / 1.05 / 2.04 ms).  The B^T tile
+    // images of the call's pre-pass live in the context's scratch.
+    unsigned char* tiles = nullptr;
+    s = SolveScratch(ctx, RoundUp(ascb_block16_tiles_bytes(a.cols, c->columns), 256), &tiles);
+    if (!s.ok()) return s;
     return Launched(ctx,
                     ascb_spmm_block16_tc(ctx->stream, &a, c->columns,
                                          static_cast<const float*>(b->data), b->leading_dimension,
                                          static_cast<float*>(const_cast<void*>(c->data)),
                                          c->leading_dimension, static_cast<float>(alpha_real),
-                                         ctx->status, ctx->sm_count),
+                                         reinterpret_cast<float*>(tiles), ctx->status,
+                                         ctx->sm_count),
                     "CUDA could not launch the tensor-core SpMM kernel");
   }
   if (!RealKind(m->element_kind)) {
@@ -1197,6 +1270,18 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
                                       c->leading_dimension, alpha_real, alpha_imag,
                                       ctx->sm_count),
                     "CUDA could not launch the complex SpMM kernel");
+  }
+  std::int64_t st_slots = 0, st_entries = 0;
+  if (!transposed && !csc && plan != nullptr && plan->use_staged &&
+      StagedApply(*plan, *b, *c, m->element_kind, ctx->device, &st_slots, &st_entries)) {
+    return Launched(ctx,
+                    ascb_spmm_staged(ctx->stream, Dtype(m->element_kind),
+                                     ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0, &a,
+                                     &plan->staged, c->columns, b->data, b->leading_dimension,
+                                     const_cast<void*>(c->data), c->leading_dimension,
+                                     alpha_real, st_slots, st_entries, ctx->status,
+                                     ctx->sm_count),
+                    "CUDA could not launch the staged SpMM kernel");
   }
   if (!transposed && !csc && plan != nullptr && plan->use_groups &&
       GroupsApply(*b, *c, m->element_kind)) {
@@ -1300,7 +1385,10 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
   if (s.ok() && (flags & ASC_SB_PLAN_ROW_GROUPS) && m->format == ASC_SB_CSR &&
       RealKind(m->element_kind) && m->rows > 0 && m->nonzeros < (std::int64_t{1} << 32)) {
     plan->groups_mem = ws + PlanLayoutFor(*m, flags).groups;
-    s = BuildRowGroups(ctx, plan, kDefaultRowsPerGroup);
+    plan->staged_mem = ws + PlanLayoutFor(*m, flags).staged;
+    s = BuildRowGroups(ctx, plan, 16);
+    if (s.ok()) s = BuildStaged(ctx, plan);
+    if (s.ok() && kDefaultRowsPerGroup != 16) s = BuildRowGroups(ctx, plan, kDefaultRowsPerGroup);
   }
   if (s.ok() && ctx->selector != nullptr && ctx->determinism != ASC_SB_DETERMINISTIC &&
       ctx->variant == ASC_SB_VARIANT_AUTO && RealKind(m->element_kind)) {
@@ -1960,7 +2048,8 @@ int asc_sb_plan_properties(const asc_sb_plan* plan, int32_t* properties) {
   if (plan == nullptr || properties == nullptr) return ASC_SB_INVALID_ARGUMENT;
   *properties = (plan->t_ptr != nullptr ? ASC_SB_PLAN_HAS_TRANSPOSE : 0) |
                 (plan->block16 ? ASC_SB_PLAN_HAS_BLOCKS16 : 0) |
-                (plan->use_groups ? ASC_SB_PLAN_HAS_ROW_GROUPS : 0);
+                (plan->use_groups ? ASC_SB_PLAN_HAS_ROW_GROUPS : 0) |
+                (plan->use_staged ? ASC_SB_PLAN_HAS_STAGED_SPMM : 0);
   return ASC_SB_OK;
 }
 
@@ -1987,8 +2076,13 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
   std::lock_guard<std::mutex> lock(ctx->mutex);
   DeviceGuard guard(ctx->device);
   if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
-  // candidates: 0 = the row-by-row kernel, else R rows per group
-  const int candidates[] = {0, 2, 4, 8, 16, 32};
+  // candidates: 0 = the row-by-row kernel, ASC_SB_SPMM_STAGED = the
+  // TMA-staged kernel, else R rows per group
+  const int candidates[] = {0, ASC_SB_SPMM_STAGED, 2, 4, 8, 16, 32};
+  std::int64_t st_slots = 0, st_entries = 0;
+  const bool staged_ok =
+      StagedApply(*plan, *b, *c, plan->matrix.element_kind, ctx->device, &st_slots, &st_entries);
+  plan->tuned_count = 0;
   cudaEvent_t start = nullptr, stop = nullptr;
   cudaError_t e = cudaEventCreate(&start);
   if (e == cudaSuccess) e = cudaEventCreate(&stop);
@@ -1996,9 +2090,11 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
   float best_time = 0.0f;
   for (int rg : candidates) {
     if (!s.ok() || e != cudaSuccess) break;
-    if (rg != 0 && plan->groups.rows_per_group != rg) s = BuildRowGroups(ctx, plan, rg);
+    if (rg == ASC_SB_SPMM_STAGED && !staged_ok) continue;
+    if (rg > 0 && plan->groups.rows_per_group != rg) s = BuildRowGroups(ctx, plan, rg);
     if (!s.ok()) break;
-    plan->use_groups = rg != 0;
+    plan->use_groups = rg > 0;
+    plan->use_staged = rg == ASC_SB_SPMM_STAGED;
     s = StandardSpmm(ctx, plan, ASC_SB_OP_NONE, alpha, 0.0, &plan->matrix, b, c);  // warm-up
     if (s.ok()) e = cudaEventRecord(start, ctx->stream);
     for (int r = 0; r < reps && s.ok() && e == cudaSuccess; ++r) {
@@ -2008,6 +2104,11 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
     if (s.ok() && e == cudaSuccess) e = cudaEventSynchronize(stop);
     float t = 0.0f;
     if (s.ok() && e == cudaSuccess) e = cudaEventElapsedTime(&t, start, stop);
+    if (s.ok() && e == cudaSuccess && plan->tuned_count < 8) {
+      plan->tuned_candidate[plan->tuned_count] = rg;
+      plan->tuned_ms[plan->tuned_count] = t / static_cast<float>(reps);
+      ++plan->tuned_count;
+    }
     if (s.ok() && e == cudaSuccess && (best < 0 || t < best_time)) {
       best = rg;
       best_time = t;
@@ -2022,9 +2123,24 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
   if (s.ok() && best > 0 && plan->groups.rows_per_group != best) s = BuildRowGroups(ctx, plan, best);
   if (!s.ok()) return Finish(ctx, s);
   plan->use_groups = best > 0;
+  plan->use_staged = best == ASC_SB_SPMM_STAGED;
   *best_ms = best_time / static_cast<float>(reps);
   *rows_per_group = best;
   return Finish(ctx, Status::Ok());
+}
+
+int asc_sb_plan_spmm_tuning(const asc_sb_plan* plan, int32_t capacity, int32_t* count,
+                            int32_t* candidates, float* ms) {
+  if (plan == nullptr || count == nullptr || capacity < 0 ||
+      (capacity > 0 && (candidates == nullptr || ms == nullptr))) {
+    return ASC_SB_INVALID_ARGUMENT;
+  }
+  *count = plan->tuned_count;
+  for (int i = 0; i < plan->tuned_count && i < capacity; ++i) {
+    candidates[i] = plan->tuned_candidate[i];
+    ms[i] = plan->tuned_ms[i];
+  }
+  return ASC_SB_OK;
 }
 
 int asc_sb_plan_autotune(asc_sb_context* ctx, asc_sb_plan* plan, const asc_sb_vector* x,

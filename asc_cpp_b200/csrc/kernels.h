@@ -180,10 +180,13 @@ int ascb_complex_spmm(void* stream, int dtype, int mode, int conj, const ascb_cs
 int ascb_block16_check(void* stream, const ascb_csr* a, int* bad, int sm_count);
 size_t ascb_block16_tc_smem(void);
 // C += alpha * A * B, row-major B (ldb) and C (ldc); values 16-byte aligned;
-// 3xTF32 on tcgen05.  status (nullable) receives 1 if a bounded wait gave up.
+// 3xTF32 on tcgen05.  `tiles`: ascb_block16_tiles_bytes(a->cols, k) device
+// bytes, 256-byte aligned, for the B^T tile images the call's pre-pass
+// writes.  status (nullable) receives 1 if a bounded wait gave up.
+size_t ascb_block16_tiles_bytes(int64_t cols, int64_t k);
 int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, const float* b,
-                         int64_t ldb, float* c, int64_t ldc, float alpha, int* status,
-                         int sm_count);
+                         int64_t ldb, float* c, int64_t ldc, float alpha, float* tiles,
+                         int* status, int sm_count);
 
 // ---- Level-1 on an indexed vector (internal_sparse_cuda::StandardOperation) ----
 enum { ASCB_L1_DOT = 0, ASCB_L1_AXPY = 1, ASCB_L1_GATHER = 2, ASCB_L1_GATHER_ZERO = 3,
@@ -269,6 +272,52 @@ int ascb_row_groups_build(void* stream, const ascb_csr* a, int elem_bytes, int r
 int ascb_spmm_groups(void* stream, int dtype, int exact, const ascb_csr* a,
                      const ascb_row_groups* rg, int64_t k, const void* b, int64_t ldb, void* c,
                      int64_t ldc, double alpha, int sm_count);
+
+// Exclusive scan of n int64 values: out[i] = in[0] + ... + in[i-1] for
+// i <= n (out holds n + 1); `sums`: (n / 2048 + 2) int64 of scratch.
+int ascb_scan_i64(void* stream, const int64_t* in, int64_t n, int64_t* out, int64_t* sums);
+
+// ---- TMA-staged SpMM (plan-built groups of 16 rows) ----
+// Per group of 16 rows: its distinct columns ("slots", column order), their
+// maximal runs of consecutive columns ("segments"), and per stored entry the
+// slot of its column.
+typedef struct ascb_staged_spmm {
+  int64_t groups;
+  int64_t* group_runs;  // [groups + 1] slots before each group
+  int64_t* group_segs;  // [groups + 1] segments before each group
+  int64_t* seg_col;     // [segments] first column
+  int64_t* seg_run;     // [segments] first slot, numbered over all groups
+  int32_t* seg_len;     // [segments] columns
+  uint16_t* slot;       // [nnz] group-relative slot of each entry's column
+  // device words: largest slot and entry counts over aligned windows of
+  // 1, 2, 4, 8, 16 groups (pairs, in that order)
+  unsigned long long* caps;
+} ascb_staged_spmm;
+typedef struct ascb_staged_layout {
+  size_t group_runs, group_segs, seg_col, seg_run, seg_len, slot, caps, persistent;
+  size_t seg_flag, seg_of, sums, total;
+} ascb_staged_layout;
+// Byte offsets in a 256-byte aligned block; [persistent, total) is build
+// scratch.
+ascb_staged_layout ascb_staged_layout_for(int64_t rows, int64_t nnz);
+// Builds the staged tables from row groups of 16 rows just built by
+// ascb_row_groups_build into `groups_base` (it reads that build's scratch).
+int ascb_staged_build(void* stream, const ascb_csr* a, const ascb_row_groups* rg16,
+                      const void* groups_base, int elem_bytes, void* base,
+                      ascb_staged_spmm* out, int sm_count);
+// Groups per pipeline stage for k right-hand sides, and the bytes of one
+// stage holding `slots` rows of B and `entries` stored entries.
+int ascb_staged_groups_per_stage(int dtype, int64_t k);
+size_t ascb_staged_stage_bytes(int dtype, int64_t k, int64_t slots, int64_t entries, int ng);
+// C += alpha * A * B (row-major B and C, rows of whole 16-byte chunks on
+// 16-byte boundaries); max_slots / max_entries: the caps of the stage width
+// ascb_staged_groups_per_stage(dtype, k); exact = 1: the reference's
+// per-entry update in stored order (bit-exact).  Two stages of
+// ascb_staged_stage_bytes each must fit one CTA's shared memory.
+int ascb_spmm_staged(void* stream, int dtype, int exact, const ascb_csr* a,
+                     const ascb_staged_spmm* st, int64_t k, const void* b, int64_t ldb, void* c,
+                     int64_t ldc, double alpha, int64_t max_slots, int64_t max_entries,
+                     int* status, int sm_count);
 
 #ifdef __cplusplus
 }

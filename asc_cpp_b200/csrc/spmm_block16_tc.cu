@@ -23,12 +23,19 @@
 // accuracy: |c - c_exact| <= (n + 64) 2^-22 |alpha| sum_k |a_k b_k| + 2^-23 |c0|
 // per output, n = stored entries in the row (tests check this bound).
 //
-// Pipeline: four producer warps each own one shared-memory stage and load,
-// split and store the blocks whose running index is their warp number mod 4;
-// a warp issues the next block's loads before it waits for its stage, so up
-// to eight blocks' loads are in flight per CTA; one thread issues the MMAs as
-// stages fill (mbarriers full / empty); two 16-column accumulators alternate
-// between block rows so the epilogue of one overlaps the MMAs of the next.
+// B tiles: a pre-pass (bt_tiles_kernel, once per product) writes, for every
+// block column and 128-column chunk of B, the two 8 KB shared-memory images
+// hi and lo of B_blk^T (zero rows past k), so a stage's B operand arrives as
+// ONE 16 KB TMA bulk copy (cp.async.bulk) from L2 -- no transposes, splits or
+// LSU traffic for B in the main kernel.
+//
+// Pipeline: four producer warps each own one shared-memory stage and fill it
+// for the blocks whose running index is their warp number mod 4: lane 0
+// issues the B tile's bulk copy (expect-tx on the stage's `full` barrier),
+// the lanes split the block's A rows (loaded before the stage wait) into
+// hi / lo and arrive; one thread issues the MMAs as stages fill (mbarriers
+// full / empty); two 16-column accumulators alternate between block rows so
+// the epilogue of one overlaps the MMAs of the next.
 // Every wait is bounded: one that runs out records 1 in *status, tells the
 // other roles to stop (a shared flag), and the CTA waits (bounded) for its own
 // MMAs before it frees its tensor memory.
@@ -56,6 +63,9 @@ struct alignas(1024) Stage {
   float a_hi[kB * kB];   // A block, 16 rows x 16 (1 KB)
   float a_lo[kB * kB];
 };
+
+static_assert(offsetof(Stage, bt_lo) == offsetof(Stage, bt_hi) + sizeof(float) * kM * kB,
+              "a stage's B^T images are adjacent: one bulk copy fills both");
 
 struct Smem {
   Stage stage[kStages];
@@ -131,6 +141,51 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
       : "memory");
 }
 
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Pre-pass: tile (bc, ch) of B^T for block column bc and right-hand sides
+// [128 ch, 128 ch + 128): element (m, kk) = B(16 bc + kk, 128 ch + m) (0 past
+// k), as the K-major 64-byte-swizzle image of a stage (hi, then lo).  One
+// thread per (tile, m, 16-byte chunk).
+constexpr int kTileFloats = kM * kB;  // 2048 per image
+__global__ void __launch_bounds__(256)
+bt_tiles_kernel(const float* __restrict__ b, int64_t ldb, int64_t k, int64_t b_rows,
+                int64_t col_blocks, int64_t chunks, float* __restrict__ tiles) {
+  const int64_t total = col_blocks * chunks * kM * 4;
+  const int64_t step = static_cast<int64_t>(gridDim.x) * blockDim.x;
+  for (int64_t i = static_cast<int64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total;
+       i += step) {
+    const int m = static_cast<int>(i % kM);
+    const int cq = static_cast<int>((i / kM) % 4);
+    const int64_t tile = i / (kM * 4);  // bc * chunks + ch
+    const int64_t bc = tile / chunks;
+    const int64_t col = (tile - bc * chunks) * kM + m;
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int64_t row = bc * kB + cq * 4 + e;
+      v[e] = col < k && row < b_rows ? __ldg(b + row * ldb + col) : 0.0f;
+    }
+    float4 hi, lo;
+    split(make_float4(v[0], v[1], v[2], v[3]), hi, lo);
+    unsigned char* base = reinterpret_cast<unsigned char*>(tiles + tile * 2 * kTileFloats);
+    *reinterpret_cast<float4*>(base + swz(m, cq)) = hi;
+    *reinterpret_cast<float4*>(base + kTileFloats * 4 + swz(m, cq)) = lo;
+  }
+}
+
 // bounded wait for phase `parity` of `bar`; false if it ran out or another
 // role of the CTA gave up (*abort)
 __device__ __forceinline__ bool wait_bar(uint64_t* bar, uint32_t parity, const int* abort) {
@@ -169,9 +224,9 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&d)[16]) {
 // arrive on dempty[a] (128 arrivals).
 __global__ void __launch_bounds__(kThreads)
 block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
-                  const float* __restrict__ val, int64_t block_rows, const float* __restrict__ b,
-                  int64_t ldb, float* __restrict__ c, int64_t ldc, int64_t k, float alpha,
-                  int* status) {
+                  const float* __restrict__ val, int64_t block_rows,
+                  const float* __restrict__ tiles, float* __restrict__ c, int64_t ldc, int64_t k,
+                  float alpha, int* status) {
   extern __shared__ unsigned char smem_raw[];
   Smem& s = *reinterpret_cast<Smem*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~static_cast<uintptr_t>(1023));
@@ -198,13 +253,6 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  // zero the B^T tiles once: rows at or beyond the chunk width stay zero
-  for (int i = t; i < kStages * 2 * kM * kB / 4; i += kThreads) {
-    float4* p = reinterpret_cast<float4*>(&s.stage[i / (2 * kM * kB / 4)].bt_hi[0]) +
-                i % (2 * kM * kB / 4);
-    *p = make_float4(0.f, 0.f, 0.f, 0.f);
-  }
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
@@ -217,8 +265,7 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
     // ---------------- producers ----------------
     const int p = warp;
     unsigned char* stage = reinterpret_cast<unsigned char*>(&s.stage[p]);
-    unsigned char* bt_hi = stage + offsetof(Stage, bt_hi);
-    unsigned char* bt_lo = stage + offsetof(Stage, bt_lo);
+    unsigned char* bt_hi = stage + offsetof(Stage, bt_hi);  // bt_lo follows it
     unsigned char* a_hi = stage + offsetof(Stage, a_hi);
     unsigned char* a_lo = stage + offsetof(Stage, a_lo);
     // this lane's A chunks: rows lane/4 and lane/4 + 8, 16-byte chunk lane%4
@@ -227,7 +274,8 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
     uint32_t it = 0, itm = 0, uses = 0;
     for (int64_t item = blockIdx.x; item < items && !failed; item += gridDim.x) {
       const int64_t br = item / chunks;
-      const int64_t m0 = (item - br * chunks) * kM;
+      const int64_t ch = item - br * chunks;
+      const int64_t m0 = ch * kM;
       const int64_t width = k - m0 < kM ? k - m0 : kM;
       const int64_t p0 = __ldg(ptr + br * kB);
       const int64_t nblk = (__ldg(ptr + br * kB + 1) - p0) / kB;
@@ -236,24 +284,20 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
       const float* a1 = val + __ldg(ptr + br * kB + ar + 8) + ac * 4;
       for (int64_t j = 0; j < nblk; ++j, ++it) {
         if ((it & 3u) != static_cast<uint32_t>(p)) continue;
-        // the block's loads go out before the wait for the stage, so their
+        // the block's A loads go out before the wait for the stage, so their
         // latency overlaps the MMAs still reading it
         const int64_t bc = __ldg(idx + p0 + j * kB) >> 4;
         const float4 va0 = __ldg(reinterpret_cast<const float4*>(a0 + j * kB));
         const float4 va1 = __ldg(reinterpret_cast<const float4*>(a1 + j * kB));
-        const float* brow = b + bc * kB * ldb + m0;
-        float bv[4][kB];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int m = lane + 32 * i;
-#pragma unroll
-          for (int kk = 0; kk < kB; ++kk) {
-            bv[i][kk] = m < width ? __ldg(brow + kk * ldb + m) : 0.0f;
-          }
-        }
         if (uses > 0 && !wait_bar(&s.empty[p], (uses - 1) & 1u, &s.abort)) {
           failed = true;
           break;
+        }
+        if (lane == 0) {
+          // B^T hi and lo of (bc, ch): one bulk copy into the stage
+          mbar_expect_tx(&s.full[p], 2 * kTileFloats * 4);
+          bulk_copy(bt_hi, tiles + (bc * chunks + ch) * 2 * kTileFloats, 2 * kTileFloats * 4,
+                    &s.full[p]);
         }
         float4 hi, lo;
         split(va0, hi, lo);
@@ -262,20 +306,6 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
         split(va1, hi, lo);
         *reinterpret_cast<float4*>(a_hi + swz(ar + 8, ac)) = hi;
         *reinterpret_cast<float4*>(a_lo + swz(ar + 8, ac)) = lo;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const int m = lane + 32 * i;
-          if (m < width) {
-#pragma unroll
-            for (int ch = 0; ch < 4; ++ch) {
-              split(make_float4(bv[i][ch * 4], bv[i][ch * 4 + 1], bv[i][ch * 4 + 2],
-                                bv[i][ch * 4 + 3]),
-                    hi, lo);
-              *reinterpret_cast<float4*>(bt_hi + swz(m, ch)) = hi;
-              *reinterpret_cast<float4*>(bt_lo + swz(m, ch)) = lo;
-            }
-          }
-        }
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         mbar_arrive(&s.full[p]);
         ++uses;
@@ -414,11 +444,29 @@ extern "C" int ascb_block16_check(void* stream, const ascb_csr* a, int* bad, int
 
 extern "C" size_t ascb_block16_tc_smem(void) { return sizeof(ascb::Smem) + 1024; }
 
+extern "C" size_t ascb_block16_tiles_bytes(int64_t cols, int64_t k) {
+  const int64_t chunks = (k + ascb::kM - 1) / ascb::kM;
+  return static_cast<size_t>((cols + ascb::kB - 1) / ascb::kB) * static_cast<size_t>(chunks) * 2 *
+         ascb::kTileFloats * sizeof(float);
+}
+
 extern "C" int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, const float* b,
                                     int64_t ldb, float* c, int64_t ldc, float alpha,
-                                    int* status, int sm_count) {
+                                    float* tiles, int* status, int sm_count) {
   using namespace ascb;
   if (a->rows <= 0 || k <= 0) return 0;
+  const int64_t col_blocks = (a->cols + kB - 1) / kB;  // B rows past cols read as 0
+  const int64_t chunks = (k + kM - 1) / kM;
+  if (col_blocks > 0) {
+    const int64_t work = col_blocks * chunks * kM * 4;
+    int64_t blocks = (work + 255) / 256;
+    const int64_t cap = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * 8;
+    if (blocks > cap) blocks = cap;
+    bt_tiles_kernel<<<static_cast<unsigned>(blocks), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        b, ldb, k, a->cols, col_blocks, chunks, tiles);
+    const cudaError_t pe = cudaGetLastError();
+    if (pe != cudaSuccess) return static_cast<int>(pe);
+  }
   const size_t smem = ascb_block16_tc_smem();
   cudaError_t e = cudaFuncSetAttribute(
       block16_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
@@ -429,7 +477,7 @@ extern "C" int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, 
   }
   if (e != cudaSuccess) return static_cast<int>(e);
   const int64_t block_rows = a->rows / 16;
-  const int64_t items = block_rows * ((k + kM - 1) / kM);
+  const int64_t items = block_rows * chunks;
   // CTAs per SM: the shared-memory limit (three at 75 KB each); the register
   // file (126 x 160 per CTA) allows more
   int device = 0, sm_smem = 0, reserved = 0;
@@ -447,7 +495,7 @@ extern "C" int ascb_spmm_block16_tc(void* stream, const ascb_csr* a, int64_t k, 
   const int64_t cap = static_cast<int64_t>(sm_count > 0 ? sm_count : 148) * per_sm;
   const unsigned grid = static_cast<unsigned>(items < cap ? (items > 0 ? items : 1) : cap);
   block16_tc_kernel<<<grid, kThreads, smem, static_cast<cudaStream_t>(stream)>>>(
-      a->ptr, a->idx, static_cast<const float*>(a->val), block_rows, b, ldb, c, ldc, k, alpha,
+      a->ptr, a->idx, static_cast<const float*>(a->val), block_rows, tiles, c, ldc, k, alpha,
       status);
   return static_cast<int>(cudaGetLastError());
 }

@@ -447,6 +447,19 @@ int ascb_row_groups_build(void* stream, const ascb_csr* a, int elem_bytes, int r
   return static_cast<int>(cudaGetLastError());
 }
 
+int ascb_scan_i64(void* stream, const int64_t* in, int64_t n, int64_t* out, int64_t* sums) {
+  if (n <= 0) {
+    return static_cast<int>(cudaMemsetAsync(out, 0, 8, static_cast<cudaStream_t>(stream)));
+  }
+  auto s = static_cast<cudaStream_t>(stream);
+  const int64_t blocks = (n + ascb::kScanItems - 1) / ascb::kScanItems;
+  ascb::scan_sums_kernel<<<static_cast<unsigned>(blocks), ascb::kThreads, 0, s>>>(in, n, sums);
+  ascb::scan_block_sums_kernel<<<1, 32, 0, s>>>(sums, blocks);
+  ascb::scan_final_kernel<<<static_cast<unsigned>(blocks), ascb::kThreads, 0, s>>>(in, n, sums,
+                                                                                 out);
+  return static_cast<int>(cudaGetLastError());
+}
+
 int ascb_spmm_groups(void* stream, int dtype, int exact, const ascb_csr* a,
                      const ascb_row_groups* rg, int64_t k, const void* b, int64_t ldb, void* c,
                      int64_t ldc, double alpha, int sm_count) {

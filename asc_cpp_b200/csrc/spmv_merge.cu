@@ -48,7 +48,7 @@ constexpr int kPerLane = kItems / 32;    // merge items per lane
 constexpr int kPad = 4;                  // alignment slack, elements
 constexpr int kStages = 2;
 constexpr uint32_t kWaitLimit = 1u << 20;  // polls before a wait gives up
-constexpr uint32_t kSuspendNs = 2000;      // hardware suspend per poll
+constexpr uint32_t kSuspendNs = tma::kTmaSuspendNs;  // stage-wait suspend hint
 constexpr int kMaxDevices = 64;
 
 // Every TMA destination starts on a 16-byte boundary; each array has room for
@@ -61,83 +61,7 @@ struct alignas(16) Stage {
   alignas(16) uint64_t bar;                    // mbarrier of this stage
 };
 
-// ---- TMA bulk copy and mbarrier primitives --------------------------------
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile(
-      "{\n .reg .b64 st;\n"
-      " mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(smem_addr(bar)),
-      "r"(bytes)
-      : "memory");
-}
-// try_wait with a suspend-time hint: the warp sleeps in hardware (up to the
-// hint, in ns) instead of re-issuing the poll.
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n"
-      " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(ok)
-      : "r"(smem_addr(bar)), "r"(parity), "r"(kSuspendNs)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes,
-                                         uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::
-          "r"(smem_addr(dst)),
-      "l"(src), "r"(bytes), "r"(smem_addr(bar))
-      : "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-}
-
-// A bulk copy of elements [first, first + count) of an array of `total`
-// elements of size E: the 16-byte aligned part goes through TMA into
-// dst + (first - aligned first); `tail` elements at the very end of the array
-// that a 16-byte rounded copy would overrun are fetched by plain loads.
-template <int E>
-struct CopyPlan {
-  int64_t g0;        // first element copied by TMA (16-byte aligned)
-  uint32_t bytes;    // TMA bytes (multiple of 16, may be 0)
-  int lead;          // smem slot of element `first`
-  int64_t tail0;     // first element loaded by plain loads
-  int tail;          // number of such elements
-};
-
-template <int E>
-__device__ __forceinline__ CopyPlan<E> plan_copy(int64_t first, int64_t count, int64_t total) {
-  constexpr int64_t kPer16 = 16 / E;
-  CopyPlan<E> c;
-  if (count <= 0) {
-    c.g0 = first;
-    c.bytes = 0;
-    c.lead = 0;
-    c.tail0 = first;
-    c.tail = 0;
-    return c;
-  }
-  c.g0 = first / kPer16 * kPer16;
-  c.lead = static_cast<int>(first - c.g0);
-  int64_t end = (first + count + kPer16 - 1) / kPer16 * kPer16;
-  int64_t safe_end = total / kPer16 * kPer16;  // last full 16-byte chunk
-  if (end > safe_end) end = safe_end > c.g0 ? safe_end : c.g0;
-  c.bytes = static_cast<uint32_t>((end - c.g0) * E);
-  c.tail0 = end;
-  c.tail = static_cast<int>(first + count > end ? first + count - end : 0);
-  return c;
-}
+using namespace tma;
 
 template <bool EXACT, bool STANDARD, typename T>
 __device__ __forceinline__ T product(T alpha, T v, T xv) {
@@ -222,12 +146,12 @@ merge_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
   // copy this warp still has in flight one more bounded wait, and report.
   auto wait = [&](int si) -> bool {
     uint32_t n = 0;  // the loop condition is warp-uniform, so is the outcome
-    while (!__all_sync(0xffffffffu, mbar_try_wait(&st[si].bar, (phase_bits >> si) & 1u))) {
+    while (!__all_sync(0xffffffffu, mbar_try_wait(&st[si].bar, (phase_bits >> si) & 1u, kSuspendNs))) {
       if (++n >= kWaitLimit) {
         if (lane == 0 && status != nullptr) atomicOr(status, 1);
         for (int k = 0; k < kStages; ++k) {
           if (!((pending_bits >> k) & 1u)) continue;
-          for (uint32_t m = 0; m < kWaitLimit && !mbar_try_wait(&st[k].bar, (phase_bits >> k) & 1u);
+          for (uint32_t m = 0; m < kWaitLimit && !mbar_try_wait(&st[k].bar, (phase_bits >> k) & 1u, kSuspendNs);
                ++m) {
           }
         }

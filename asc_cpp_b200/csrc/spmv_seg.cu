@@ -1,26 +1,27 @@
 // Register-segmented CSR SpMV for sm_100a (the default SpMV kernel, both
 // numerical modes).
 //
-// Tiles are the warp row tiles of the partition kernel (weight W = 8, 256
-// weighted items: at most 32 rows, all but the last shorter than 256
-// nonzeros).  For one tile:
-//   * the window of at most 256 nonzero positions is split into 32 lanes x 8
-//     CONTIGUOUS positions, so each lane fetches its column indices and values
-//     with 128-bit vector loads (every sector fully used) straight into
-//     registers and keeps 8 independent x gathers in flight;
-//   * a 256-bit shared bitmap marks the positions where rows start; each lane
-//     runs a segmented sum over its 8 products, closing a row at every start;
-//   * rows that cross lane boundaries are joined, and the lane that holds a
-//     row's last product writes y:
-//       FAST  -- one segmented warp scan of the lanes' open partial sums;
-//                |y - y_ref| <= gamma_{n+2}(|alpha||A||x| + |beta||y|);
-//       EXACT -- the running sum is handed lane to lane in stored order (a
-//                lane waits only if its first position continues a row), so
-//                every row is summed exactly as the serial reference does.
-// No shared-memory product buffer, no per-row loop: lane utilisation does not
-// depend on the row-length distribution.  The last row of a tile may be long;
-// its remainder past the window is reduced by the whole warp (EXACT: in
-// stored order by one lane).
+// Row tiles: tile k holds the rows r with W*r + ptr[r] in [I*k, I*(k+1)):
+// the warp tiles (W = 8, I = 256: at most 32 rows) or the kernel's own tiles
+// (W = 2, I = 251: at most 125 rows, so short rows leave less of each window
+// empty).  For one tile:
+//   * the window -- at most 256 nonzero positions from the aligned position
+//     at or before the tile's first nonzero -- is split into 32 lanes x 8
+//     CONTIGUOUS positions; each lane fetches its column indices and values
+//     with 16- or 32-byte vector loads straight into registers (every sector
+//     touched once with 32-byte loads) and keeps 8 x gathers in flight;
+//   * FAST: a 256-bit shared bitmap marks the positions where rows start,
+//     each lane runs a segmented sum over its 8 products, and one segmented
+//     warp scan joins the rows that cross lanes;
+//     |y - y_ref| <= gamma_{n+2}(|alpha||A||x| + |beta||y|);
+//   * EXACT: the products are formed in parallel and kept in shared memory,
+//     then lane k adds the products of the tile's rows k, k + 32, ... in
+//     stored order -- every row is summed exactly as the serial reference
+//     does, all rows of the tile at once.
+// Every row of a tile but the last ends inside its window; the last may run
+// on, and its remainder is reduced by the whole warp in rounds of 256
+// (EXACT: added in stored order by its lane; ROW_SPLIT: long tails handed to
+// a second kernel).
 #include "common.cuh"
 #include "kernels.h"
 

@@ -453,8 +453,9 @@ class CsrPlan:
     def spmm_autotune(self, alpha: float, b: "DenseMatrixView", c: "DenseMatrixView",
                       reps: int = 5) -> tuple[float, int]:
         """Times the SpMM kernels on these operands (C accumulates) and keeps
-        the fastest; returns (ms per product, rows per group, 0 = row by row).
-        Needs a plan created with PLAN_ROW_GROUPS."""
+        the fastest; returns (ms per product, rows per group: 0 = row by row,
+        SPMM_STAGED = the TMA-staged kernel).  Needs a plan created with
+        PLAN_ROW_GROUPS."""
         bd, cd = b.describe(), c.describe()
         bd.writable = 0
         ms = ctypes.c_float()
@@ -463,6 +464,16 @@ class CsrPlan:
             self.context.handle, self._h, float(alpha), ctypes.byref(bd), ctypes.byref(cd),
             reps, ctypes.byref(ms), ctypes.byref(rg)))
         return ms.value, rg.value
+
+    def spmm_tuning(self) -> dict[int, float]:
+        """The last spmm_autotune's table: {candidate: ms per product}."""
+        count = ctypes.c_int32()
+        cands = (ctypes.c_int32 * 8)()
+        ms = (ctypes.c_float * 8)()
+        rc = self.context._lib.asc_sb_plan_spmm_tuning(self._h, 8, ctypes.byref(count), cands, ms)
+        if rc != 0:
+            raise AscError(rc, "asc_sb_plan_spmm_tuning failed")
+        return {int(cands[i]): float(ms[i]) for i in range(min(count.value, 8))}
 
     def csr_spmv(self, alpha: float, x: CudaStridedVectorView, beta: float,
                  y: CudaStridedVectorView) -> None:

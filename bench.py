@@ -708,7 +708,8 @@ def run_extra(args):
         for name, det in (("deterministic", Determinism.kDeterministic),
                           ("default", Determinism.kBackendDefault)):
             ctx.set_determinism(det)
-            y.zero_()
+            with torch.cuda.stream(stream):  # ordered before the product
+                y.zero_()
             sc.CudaSpmv(ctx, op, 1.0, A, xv, yv, plan=plan)
             stream.synchronize()
             got[name] = y.cpu().numpy()
@@ -731,42 +732,54 @@ def run_extra(args):
         flops = 2 * a_h.nnz * k
         bv = sc.DenseMatrixView(B, a_h.cols, k, writable=False)
         cv = sc.DenseMatrixView(C, a_h.rows, k)
-        from asc_cpp_b200._abi import PLAN_HAS_ROW_GROUPS, PLAN_ROW_GROUPS
+        from asc_cpp_b200._abi import PLAN_HAS_ROW_GROUPS, PLAN_HAS_STAGED_SPMM, PLAN_ROW_GROUPS
         # a plan detects dense 16 x 16 blocks (tensor-core path) and builds the
-        # row groups (B rows shared by neighbouring rows)
+        # TMA-staged tables and row groups (B rows shared by neighbouring rows)
+        t0 = time.time()
         plan = sc.CsrPlan(ctx, A, PLAN_ROW_GROUPS)
+        stream.synchronize()
+        extra_cfg["plan_create_s"] = round(time.time() - t0, 3)
         extra_cfg["dense_blocks16"] = bool(plan.properties() & 2)
         extra_cfg["row_groups_kept"] = bool(plan.properties() & PLAN_HAS_ROW_GROUPS)
+        extra_cfg["staged_kept"] = bool(plan.properties() & PLAN_HAS_STAGED_SPMM)
         plain = sc.CsrPlan(ctx, A)
+        plan_tag = "_staged" if extra_cfg["staged_kept"] else "_row_groups"
         for name, det in (("deterministic", Determinism.kDeterministic),
                           ("default", Determinism.kBackendDefault)):
             ctx.set_determinism(det)
-            for tag, p_ in (("", plain), ("_row_groups", plan)):
+            for tag, p_ in (("", plain), (plan_tag, plan)):
                 ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv,
                                                plan=p_))
                 detail[name + tag] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
                                       "gflops": round(flops / ms / 1e6, 1)}
-            # the SpMM autotuner on this k (row by row, or R rows per group)
-            scratch = torch.zeros_like(C)
-            t_ms, rg = plan.spmm_autotune(1.0, bv, sc.DenseMatrixView(scratch, a_h.rows, k), 5)
-            ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv,
-                                           plan=plan))
-            detail[name + "_autotuned"] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
-                                           "gflops": round(flops / ms / 1e6, 1),
-                                           "rows_per_group": rg}
-            del scratch
-        # the fastest default-mode product against the FP64 oracle on a row
-        # sample (the checker; after every timed region)
-        best_default = min((kk for kk in detail if kk.startswith("default")),
-                           key=lambda kk: detail[kk]["ms"])
-        ctx.set_determinism(Determinism.kBackendDefault)
+        # the faster default-mode path (plain or the plan's) against the FP64
+        # oracle on a row sample (the checker; after the timed regions, before
+        # the autotuner changes the plan)
+        best_default = min(("default", "default" + plan_tag), key=lambda kk: detail[kk]["ms"])
         use = plain if best_default == "default" else plan
-        C.zero_()
+        with torch.cuda.stream(stream):  # ordered before the product
+            C.zero_()
         sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv, plan=use)
         stream.synchronize()
         extra_cfg["error_vs_fp64_oracle"] = spmm_error(a_h, B.cpu().numpy(), C.cpu().numpy(),
                                                        best_default, 65_536,
                                                        extra_cfg["dense_blocks16"])
+        # the SpMM autotuner on this k (row by row, staged, or R rows per
+        # group), per mode
+        for name, det in (("deterministic", Determinism.kDeterministic),
+                          ("default", Determinism.kBackendDefault)):
+            ctx.set_determinism(det)
+            with torch.cuda.stream(stream):
+                scratch = torch.zeros_like(C)
+            t_ms, rg = plan.spmm_autotune(1.0, bv, sc.DenseMatrixView(scratch, a_h.rows, k), 5)
+            ms = timed(lambda: sc.CudaSpmm(ctx, SparseBlasTranspose.kNone, 1.0, A, bv, cv,
+                                           plan=plan))
+            detail[name + "_autotuned"] = {"ms": round(ms, 4), "gbs": round(byts / ms / 1e6, 1),
+                                           "gflops": round(flops / ms / 1e6, 1),
+                                           "rows_per_group": rg,
+                                           "tuning_ms": {str(kk): round(vv, 4) for kk, vv in
+                                                         plan.spmm_tuning().items()}}
+            del scratch
         plan.close()
         plain.close()
         dtype_s = "f32"
@@ -813,12 +826,16 @@ def run_extra(args):
         # (a device copy of n elements, inside the timed region)
         byts = a_h.nnz * (es + 8) + (n + 1) * 8 + 2 * n * es
 
+        def restore():
+            with torch.cuda.stream(stream):  # the library's stream, ahead of the solve
+                xb.copy_(b0)
+
         def solve(use_plan):
-            xb.copy_(b0)
+            restore()
             sc.CudaSparseTriangularSolveMultiple(ctx, SparseBlasTranspose.kNone, 1.0, A,
                                                  SparseBlasTriangle.kLower, diag, rhs,
                                                  plan=plan if use_plan else None)
-        copy_ms = timed(lambda: xb.copy_(b0))
+        copy_ms = timed(restore)
         for name, det, use_plan in (("deterministic", Determinism.kDeterministic, False),
                                     ("default", Determinism.kBackendDefault, False)):
             ctx.set_determinism(det)

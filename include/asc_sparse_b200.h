@@ -380,15 +380,23 @@ ASC_SB_API int asc_sb_clone_indexed(asc_sb_context* context,
 /* ASC_SB_PLAN_TRIANGULAR adds the ready flags of triangular solves
  * (asc_sb_plan_triangular_solve); solves through one plan must be ordered
  * (one stream). */
-/* ASC_SB_PLAN_ROW_GROUPS (CSR, float or double) merges the column lists of
- * every R consecutive rows (R = 8 at creation; asc_sb_plan_spmm_autotune may
- * choose another) into runs -- one per distinct column, with the rows that
- * hold it -- so that asc_sb_plan_standard_spmm (op = none, row-major B and C
- * with 16-byte aligned rows) loads each row of B once per run and applies it
- * to all of the run's rows.  Each row still adds its entries in stored
- * order: DETERMINISTIC results stay bit-identical to the reference.  The
- * groups are used when they share B rows (at least 1.25 entries per run) or
- * when the autotuner found them faster. */
+/* ASC_SB_PLAN_ROW_GROUPS (CSR, float or double) prepares two SpMM paths for
+ * asc_sb_plan_standard_spmm with op = none and row-major B and C whose rows
+ * are whole 16-byte chunks on 16-byte boundaries:
+ *   - the TMA-staged kernel: per group of 16 rows, the distinct columns in
+ *     runs of consecutive columns and per stored entry the slot of its
+ *     column; each CTA stages a group's rows of B, row offsets, values and
+ *     slots in shared memory with bulk copies (two-stage pipeline) and
+ *     computes from there.  Used when the groups share columns (at least 1.25
+ *     entries per distinct column) and two stages fit one CTA's shared
+ *     memory for the call's k;
+ *   - row groups of R rows (R = 8 at creation; asc_sb_plan_spmm_autotune may
+ *     choose another): runs -- one per distinct column, with the rows that
+ *     hold it -- so that each row of B is loaded once per run and applied to
+ *     all of the run's rows; used when they share B rows (at least 1.25
+ *     entries per run) or when the autotuner found them faster.
+ * Either way each row adds its entries in stored order: DETERMINISTIC results
+ * stay bit-identical to the reference. */
 enum { ASC_SB_PLAN_TRANSPOSE = 1, ASC_SB_PLAN_TRIANGULAR = 2, ASC_SB_PLAN_ROW_GROUPS = 4 };
 typedef struct asc_sb_plan asc_sb_plan;
 ASC_SB_API int asc_sb_plan_workspace_size(asc_sb_context* context,
@@ -424,7 +432,8 @@ ASC_SB_API int asc_sb_plan_standard_spmv(asc_sb_context* context,
  * |c - c_exact| <= (n + 64) 2^-22 |alpha| sum_k |a_k b_k| + 2^-23 |c0| per
  * output (n = stored entries of the row). */
 enum { ASC_SB_PLAN_HAS_TRANSPOSE = 1, ASC_SB_PLAN_HAS_BLOCKS16 = 2,
-       ASC_SB_PLAN_HAS_ROW_GROUPS = 4 /* SpMM runs through the row groups */ };
+       ASC_SB_PLAN_HAS_ROW_GROUPS = 4 /* SpMM runs through the row groups */,
+       ASC_SB_PLAN_HAS_STAGED_SPMM = 8 /* SpMM runs through the staged kernel */ };
 ASC_SB_API int asc_sb_plan_properties(const asc_sb_plan* plan,
                                       int32_t* properties);
 /* Standard SpMM through a plan: same contract as asc_sb_standard_spmm, with
@@ -437,16 +446,23 @@ ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
                                          const asc_sb_dense* output);
 /* SpMM autotuner of a plan created with ASC_SB_PLAN_ROW_GROUPS: times, on
  * these operands (C += alpha * A * B, `reps` products each plus one warm-up,
- * CUDA events on the context stream), the row-by-row kernel and the row-group
- * kernel with R = 2, 4, 8, 16 and 32 rows per group (k-tile and lanes per row
- * follow from R and k), keeps the fastest for the plan's later products and
- * returns its time per product and R (0: row by row).  The products run for
- * real, so C accumulates.  No counterpart in the reference. */
+ * CUDA events on the context stream), the row-by-row kernel, the TMA-staged
+ * kernel (where it fits) and the row-group kernel with R = 2, 4, 8, 16 and 32
+ * rows per group (k-tile and lanes per row follow from R and k), keeps the
+ * fastest for the plan's later products and returns its time per product and
+ * R (0: row by row; ASC_SB_SPMM_STAGED: the staged kernel).  The products run
+ * for real, so C accumulates.  No counterpart in the reference. */
+enum { ASC_SB_SPMM_STAGED = -1 };
 ASC_SB_API int asc_sb_plan_spmm_autotune(asc_sb_context* context,
                                          asc_sb_plan* plan, double alpha,
                                          const asc_sb_dense* input,
                                          const asc_sb_dense* output, int32_t reps,
                                          float* best_ms, int32_t* rows_per_group);
+/* The last asc_sb_plan_spmm_autotune's table: *count candidates in the order
+ * timed (R as returned by the autotuner) and their ms per product; up to
+ * `capacity` of them are copied. */
+ASC_SB_API int asc_sb_plan_spmm_tuning(const asc_sb_plan* plan, int32_t capacity,
+                                       int32_t* count, int32_t* candidates, float* ms);
 
 /* Triangular solve through a plan created with ASC_SB_PLAN_TRIANGULAR: same
  * contract as asc_sb_standard_triangular_solve on the plan's matrix; op !=

@@ -11,7 +11,7 @@ import pytest
 
 import oracle
 from asc_cpp_b200 import synthetic
-from asc_cpp_b200._abi import (PLAN_HAS_ROW_GROUPS, PLAN_ROW_GROUPS, Determinism,
+from asc_cpp_b200._abi import (PLAN_HAS_ROW_GROUPS, PLAN_ROW_GROUPS, SPMM_STAGED, Determinism,
                                SparseBlasTranspose)
 from asc_cpp_b200.sparse_cuda import CsrPlan, CudaSpmm, DenseMatrixView
 from oracle import CSR, OP_NONE, ROW_MAJOR
@@ -60,7 +60,7 @@ def test_row_groups_bit_exact_every_group_size(cuda_lib, restatement, dt, k):
         scratch = dev(c0)
         ms, rg = plan.spmm_autotune(0.5, DenseMatrixView(dev(b), a_h.cols, k, writable=False),
                                     DenseMatrixView(scratch, a_h.rows, k), reps=1)
-        assert rg in (0, 2, 4, 8, 16, 32) and ms > 0
+        assert rg in (0, SPMM_STAGED, 2, 4, 8, 16, 32) and ms > 0
         assert bits_equal(spmm(ctx, plan, a, b, c0, -1.25, k), want), (name, rg)
         plan.close()
     ctx.close()
