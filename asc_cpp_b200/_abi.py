@@ -86,7 +86,8 @@ PLAN_HAS_TRANSPOSE = 1
 PLAN_HAS_BLOCKS16 = 2
 PLAN_HAS_ROW_GROUPS = 4
 PLAN_HAS_STAGED_SPMM = 8
-SPMM_STAGED = -1  # asc_sb_plan_spmm_autotune: the TMA-staged kernel won
+SPMM_STAGED = -1  # the TMA-staged SpMM kernel (autotune result, set_spmm choice)
+SPMM_AUTO = -2    # asc_sb_plan_set_spmm: the plan's default rules
 
 
 class SparseDesc(ctypes.Structure):
@@ -217,6 +218,7 @@ SIGNATURES: dict[str, tuple] = {
     "asc_sb_plan_spmm_autotune": (ctypes.c_int, [_P, _P, _D, _DP, _DP, _I32,
                                                  ctypes.POINTER(ctypes.c_float),
                                                  ctypes.POINTER(_I32)]),
+    "asc_sb_plan_set_spmm": (ctypes.c_int, [_P, _P, _I32]),
     "asc_sb_plan_spmm_tuning": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_I32),
                                                ctypes.POINTER(_I32),
                                                ctypes.POINTER(ctypes.c_float)]),

@@ -126,8 +126,10 @@ struct asc_sb_plan {
   unsigned char* staged_mem = nullptr;
   ascb_staged_spmm staged{};
   std::int64_t staged_caps[10] = {};
+  std::int64_t staged_slots = 0;  // distinct columns over all 16-row groups
   bool has_staged = false;
-  bool use_staged = false;  // SpMM through the staged kernel where it fits
+  bool use_staged = false;    // SpMM through the staged kernel where it fits ...
+  bool staged_tuned = false;  // ... for every k (the autotuner picked it), else for 16 <= k <= 64
   // the last SpMM autotune: candidates timed and their ms per product
   int tuned_count = 0;
   int tuned_candidate[8] = {};
@@ -527,6 +529,7 @@ Status BuildStaged(asc_sb_context* ctx, asc_sb_plan* plan) {
   for (int i = 0; i < 10; ++i) plan->staged_caps[i] = static_cast<std::int64_t>(caps[i]);
   plan->has_staged = true;
   const std::int64_t slots = plan->group_run_count;  // of the 16-row groups
+  plan->staged_slots = slots;
   plan->use_staged = slots > 0 && 4 * a.nnz >= 5 * slots;
   return Status::Ok();
 }
@@ -1271,8 +1274,15 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
                                       ctx->sm_count),
                     "CUDA could not launch the complex SpMM kernel");
   }
+  // the staged kernel by default for 16 <= k <= 64 elements (on a 27-point
+  // 128^3 stencil, B200: k = 32 0.60 ms against 0.62 ms contracted and 0.62
+  // against 0.87 ms bit-exact; k = 8 0.54 against 0.31 ms -- B rows of 32
+  // bytes make the bulk copies too small; k = 128 3.1 against 1.75 ms --
+  // shared-memory reads bound it); for any k once the autotuner picked it
   std::int64_t st_slots = 0, st_entries = 0;
+  const bool staged_k = c->columns >= 16 && c->columns <= 64;
   if (!transposed && !csc && plan != nullptr && plan->use_staged &&
+      (plan->staged_tuned || staged_k) &&
       StagedApply(*plan, *b, *c, m->element_kind, ctx->device, &st_slots, &st_entries)) {
     return Launched(ctx,
                     ascb_spmm_staged(ctx->stream, Dtype(m->element_kind),
@@ -1389,6 +1399,12 @@ int asc_sb_plan_create(asc_sb_context* ctx, const asc_sb_sparse* m, int32_t flag
     s = BuildRowGroups(ctx, plan, 16);
     if (s.ok()) s = BuildStaged(ctx, plan);
     if (s.ok() && kDefaultRowsPerGroup != 16) s = BuildRowGroups(ctx, plan, kDefaultRowsPerGroup);
+    // row groups only where the autotuner measured them faster: on B200 they
+    // lose to the row-by-row kernel on stencils (27-point 128^3, k = 32:
+    // 2.2 ms with R = 8 against 0.62 ms) and win on dense-block rows in
+    // DETERMINISTIC mode (16 x 16 blocks, k = 32: 0.93 ms with R = 16
+    // against 1.29 ms)
+    plan->use_groups = false;
   }
   if (s.ok() && ctx->selector != nullptr && ctx->determinism != ASC_SB_DETERMINISTIC &&
       ctx->variant == ASC_SB_VARIANT_AUTO && RealKind(m->element_kind)) {
@@ -2086,7 +2102,8 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
   cudaEvent_t start = nullptr, stop = nullptr;
   cudaError_t e = cudaEventCreate(&start);
   if (e == cudaSuccess) e = cudaEventCreate(&stop);
-  int best = -1;
+  int best = 0;
+  bool have_best = false;
   float best_time = 0.0f;
   for (int rg : candidates) {
     if (!s.ok() || e != cudaSuccess) break;
@@ -2095,6 +2112,7 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
     if (!s.ok()) break;
     plan->use_groups = rg > 0;
     plan->use_staged = rg == ASC_SB_SPMM_STAGED;
+    plan->staged_tuned = rg == ASC_SB_SPMM_STAGED;
     s = StandardSpmm(ctx, plan, ASC_SB_OP_NONE, alpha, 0.0, &plan->matrix, b, c);  // warm-up
     if (s.ok()) e = cudaEventRecord(start, ctx->stream);
     for (int r = 0; r < reps && s.ok() && e == cudaSuccess; ++r) {
@@ -2109,9 +2127,10 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
       plan->tuned_ms[plan->tuned_count] = t / static_cast<float>(reps);
       ++plan->tuned_count;
     }
-    if (s.ok() && e == cudaSuccess && (best < 0 || t < best_time)) {
+    if (s.ok() && e == cudaSuccess && (!have_best || t < best_time)) {
       best = rg;
       best_time = t;
+      have_best = true;
     }
   }
   if (start != nullptr) (void)cudaEventDestroy(start);
@@ -2124,8 +2143,39 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
   if (!s.ok()) return Finish(ctx, s);
   plan->use_groups = best > 0;
   plan->use_staged = best == ASC_SB_SPMM_STAGED;
+  plan->staged_tuned = best == ASC_SB_SPMM_STAGED;
   *best_ms = best_time / static_cast<float>(reps);
   *rows_per_group = best;
+  return Finish(ctx, Status::Ok());
+}
+
+int asc_sb_plan_set_spmm(asc_sb_context* ctx, asc_sb_plan* plan, int32_t choice) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "null plan"));
+  if (plan->groups_mem == nullptr) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_STATE,
+                            "choosing the SpMM kernel needs a plan created with "
+                            "ASC_SB_PLAN_ROW_GROUPS"));
+  }
+  const bool valid = choice == ASC_SB_SPMM_AUTO || choice == ASC_SB_SPMM_STAGED || choice == 0 ||
+                     choice == 2 || choice == 4 || choice == 8 || choice == 16 || choice == 32;
+  if (!valid) return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "unknown SpMM kernel choice"));
+  if (choice == ASC_SB_SPMM_STAGED && !plan->has_staged) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_STATE, "the plan holds no staged SpMM tables"));
+  }
+  std::lock_guard<std::mutex> lock(ctx->mutex);
+  DeviceGuard guard(ctx->device);
+  if (!guard.ok()) return Finish(ctx, Fail(ASC_SB_UNAVAILABLE, "CUDA device is unavailable"));
+  if (choice > 0 && plan->groups.rows_per_group != choice) {
+    s = BuildRowGroups(ctx, plan, choice);
+    if (!s.ok()) return Finish(ctx, s);
+  }
+  plan->use_groups = choice > 0;
+  plan->use_staged = choice == ASC_SB_SPMM_STAGED ||
+                     (choice == ASC_SB_SPMM_AUTO && plan->has_staged &&
+                      4 * plan->matrix.nonzeros >= 5 * plan->staged_slots);
+  plan->staged_tuned = choice == ASC_SB_SPMM_STAGED;
   return Finish(ctx, Status::Ok());
 }
 

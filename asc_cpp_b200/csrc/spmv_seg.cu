@@ -91,7 +91,7 @@ struct SegSmem {
   uint32_t bits[kItems / 32 + 1];  // row-start bitmap of positions 0..256
   int16_t rowid[kMaxRows + 1];     // k-th nonempty row of the tile -> its offset
   int64_t bnd[kChunk + 1];         // first row of tiles c0 .. c0 + kChunk
-  T prod[kItems];                  // exact form: products of a long row's tail
+  alignas(16) T prod[kItems];      // exact form: the window's / a long row's products
 };
 
 // Arithmetic of the two modes.  EXACT rounds every product and sum separately
@@ -227,6 +227,30 @@ __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
   }
 }
 
+// A lane's 8 products into its 8 consecutive shared-memory slots without bank
+// conflicts.  Lane l owns bytes [8 l sizeof(T), ...): stored chunk by chunk in
+// the same order by every lane, every second (FP64) or fourth (FP32) lane
+// hits the same banks.  Lane l stores its 16-byte chunk (j + l / 2) % 4 in step
+// j instead (FP32: (j + l / 4) % 2), so 8 consecutive lanes cover all 32 banks.
+__device__ __forceinline__ void store_run(double* dst, int lane, const double (&p)[kPer]) {
+  const int h = (lane >> 1) & 3;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = (j + h) & 3;
+    double2 v;  // chunk c of p, selected without dynamic register indexing
+    v.x = c == 0 ? p[0] : c == 1 ? p[2] : c == 2 ? p[4] : p[6];
+    v.y = c == 0 ? p[1] : c == 1 ? p[3] : c == 2 ? p[5] : p[7];
+    *reinterpret_cast<double2*>(dst + 2 * c) = v;
+  }
+}
+__device__ __forceinline__ void store_run(float* dst, int lane, const float (&p)[kPer]) {
+  const bool h = ((lane >> 2) & 1) != 0;
+  const float4 lo = make_float4(p[0], p[1], p[2], p[3]);
+  const float4 hi = make_float4(p[4], p[5], p[6], p[7]);
+  *reinterpret_cast<float4*>(dst + (h ? 4 : 0)) = h ? hi : lo;
+  *reinterpret_cast<float4*>(dst + (h ? 0 : 4)) = h ? lo : hi;
+}
+
 // EXACT tile: the window's products are formed in parallel (8 contiguous
 // positions per lane, as in the contracted tile) and staged in shared memory;
 // then lane k, which holds row r0 + k's bounds, adds that row's products in
@@ -261,8 +285,7 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
   T p[kPer];
   lane_products<T, true, STANDARD, UNIT, V32>(p, vmask, idx + (a0 + p0), val + (a0 + p0), x, incx,
                                               alpha);
-#pragma unroll
-  for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = p[k];
+  store_run(w.prod + p0, lane, p);
   __syncwarp();
 
   // lane l sums rows l, l + 32, ... (tiles of more than 32 rows: the bounds of
@@ -305,8 +328,7 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
       __syncwarp();  // the previous round's products have been read
       lane_products<T, true, STANDARD, UNIT, V32>(q, (1u << hi) - 1u, idx + (q0 + p0),
                                                   val + (q0 + p0), x, incx, alpha);
-#pragma unroll
-      for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = q[k];
+      store_run(w.prod + p0, lane, q);
       __syncwarp();
       if (carries) {
         int k = 0;
@@ -532,8 +554,7 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
         for (int k = 0; k < kPer; ++k) part += q[k];
       } else {
         // stored order: lane 0 adds the round's products from shared memory
-#pragma unroll
-        for (int k = 0; k < kPer; ++k) w.prod[p0 + k] = q[k];
+        store_run(w.prod + p0, lane, q);
         __syncwarp();
         if (lane == 0) {
           int k = 0;

@@ -465,6 +465,13 @@ class CsrPlan:
             reps, ctypes.byref(ms), ctypes.byref(rg)))
         return ms.value, rg.value
 
+    def set_spmm(self, choice: int) -> None:
+        """Chooses the SpMM kernel: 0 row by row, SPMM_STAGED, R rows per
+        group (2..32), or SPMM_AUTO.  Needs a plan created with
+        PLAN_ROW_GROUPS."""
+        self.context.check(self.context._lib.asc_sb_plan_set_spmm(self.context.handle, self._h,
+                                                                   int(choice)))
+
     def spmm_tuning(self) -> dict[int, float]:
         """The last spmm_autotune's table: {candidate: ms per product}."""
         count = ctypes.c_int32()

@@ -743,7 +743,14 @@ def run_extra(args):
         extra_cfg["row_groups_kept"] = bool(plan.properties() & PLAN_HAS_ROW_GROUPS)
         extra_cfg["staged_kept"] = bool(plan.properties() & PLAN_HAS_STAGED_SPMM)
         plain = sc.CsrPlan(ctx, A)
-        plan_tag = "_staged" if extra_cfg["staged_kept"] else "_row_groups"
+        # the staged kernel at this k (where its stages fit), whatever the
+        # plan's default rule would pick
+        plan_tag = "_staged"
+        if extra_cfg["staged_kept"]:
+            from asc_cpp_b200._abi import SPMM_STAGED
+            plan.set_spmm(SPMM_STAGED)
+        else:
+            plan_tag = "_plan_default"
         for name, det in (("deterministic", Determinism.kDeterministic),
                           ("default", Determinism.kBackendDefault)):
             ctx.set_determinism(det)

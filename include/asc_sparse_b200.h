@@ -380,22 +380,21 @@ ASC_SB_API int asc_sb_clone_indexed(asc_sb_context* context,
 /* ASC_SB_PLAN_TRIANGULAR adds the ready flags of triangular solves
  * (asc_sb_plan_triangular_solve); solves through one plan must be ordered
  * (one stream). */
-/* ASC_SB_PLAN_ROW_GROUPS (CSR, float or double) prepares two SpMM paths for
- * asc_sb_plan_standard_spmm with op = none and row-major B and C whose rows
- * are whole 16-byte chunks on 16-byte boundaries:
+/* ASC_SB_PLAN_ROW_GROUPS (CSR, float or double) prepares two more SpMM
+ * kernels for asc_sb_plan_standard_spmm with op = none and row-major B and C
+ * whose rows are whole 16-byte chunks on 16-byte boundaries:
  *   - the TMA-staged kernel: per group of 16 rows, the distinct columns in
  *     runs of consecutive columns and per stored entry the slot of its
- *     column; each CTA stages a group's rows of B, row offsets, values and
- *     slots in shared memory with bulk copies (two-stage pipeline) and
- *     computes from there.  Used when the groups share columns (at least 1.25
- *     entries per distinct column) and two stages fit one CTA's shared
- *     memory for the call's k;
- *   - row groups of R rows (R = 8 at creation; asc_sb_plan_spmm_autotune may
- *     choose another): runs -- one per distinct column, with the rows that
- *     hold it -- so that each row of B is loaded once per run and applied to
- *     all of the run's rows; used when they share B rows (at least 1.25
- *     entries per run) or when the autotuner found them faster.
- * Either way each row adds its entries in stored order: DETERMINISTIC results
+ *     column; a producer warp per CTA stages a group's rows of B, row
+ *     offsets, values and slots in shared memory with bulk copies (two-stage
+ *     pipeline) and the other warps compute from there.  By default it runs
+ *     when the groups share columns (at least 1.25 entries per distinct
+ *     column), 16 <= k <= 64 and two stages fit one CTA's shared memory;
+ *   - row groups of R rows (R = 8 at creation): runs -- one per distinct
+ *     column, with the rows that hold it -- so that each row of B is loaded
+ *     once per run and applied to all of the run's rows.  Used only when
+ *     chosen: by asc_sb_plan_spmm_autotune or asc_sb_plan_set_spmm.
+ * Every kernel adds each row's entries in stored order: DETERMINISTIC results
  * stay bit-identical to the reference. */
 enum { ASC_SB_PLAN_TRANSPOSE = 1, ASC_SB_PLAN_TRIANGULAR = 2, ASC_SB_PLAN_ROW_GROUPS = 4 };
 typedef struct asc_sb_plan asc_sb_plan;
@@ -452,7 +451,13 @@ ASC_SB_API int asc_sb_plan_standard_spmm(asc_sb_context* context,
  * fastest for the plan's later products and returns its time per product and
  * R (0: row by row; ASC_SB_SPMM_STAGED: the staged kernel).  The products run
  * for real, so C accumulates.  No counterpart in the reference. */
-enum { ASC_SB_SPMM_STAGED = -1 };
+enum { ASC_SB_SPMM_STAGED = -1, ASC_SB_SPMM_AUTO = -2 };
+/* Chooses the SpMM kernel of a plan created with ASC_SB_PLAN_ROW_GROUPS:
+ * 0 = row by row, ASC_SB_SPMM_STAGED = the TMA-staged kernel wherever it fits
+ * (any k), R = 2, 4, 8, 16 or 32 = row groups of R rows (rebuilt on the
+ * stream), ASC_SB_SPMM_AUTO = the defaults above. */
+ASC_SB_API int asc_sb_plan_set_spmm(asc_sb_context* context, asc_sb_plan* plan,
+                                    int32_t choice);
 ASC_SB_API int asc_sb_plan_spmm_autotune(asc_sb_context* context,
                                          asc_sb_plan* plan, double alpha,
                                          const asc_sb_dense* input,

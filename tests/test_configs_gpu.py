@@ -23,7 +23,8 @@ import torch
 
 import oracle
 from asc_cpp_b200 import synthetic
-from asc_cpp_b200._abi import (PLAN_HAS_BLOCKS16, PLAN_TRANSPOSE, Determinism,
+from asc_cpp_b200._abi import (PLAN_HAS_BLOCKS16, PLAN_HAS_STAGED_SPMM, PLAN_ROW_GROUPS,
+                               PLAN_TRANSPOSE, SPMM_STAGED, Determinism,
                                SparseBlasTranspose, Variant)
 from asc_cpp_b200.sparse_cuda import (CsrPlan, CudaBatch, CudaCsrArray, CudaCsrSpmv,
                                       CudaCsrSpmvWorkspaceSize, CudaSpmm, CudaSpmv,
@@ -182,6 +183,12 @@ def test_stencil_128_spmm(cuda_lib, restatement, k):
     want = oracle.standard_spmm_rows(restatement, a_h.cols, a_h.ptr, a_h.idx, a_h.val, alpha, b,
                                      np.zeros((a_h.rows, k), np.float32))
     assert bits_equal(got, want)
+    # the TMA-staged kernel (16-row groups) at full size, bit for bit too
+    staged = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+    assert staged.properties() & PLAN_HAS_STAGED_SPMM
+    staged.set_spmm(SPMM_STAGED)
+    assert bits_equal(run_spmm(ctx, a, b_d, a_h.rows, a_h.cols, k, alpha, staged), want)
+    staged.close()
     del got, want
     ctx.set_determinism(Determinism.kBackendDefault)
     for use_plan in (False, True):

@@ -11,9 +11,9 @@ import pytest
 
 import oracle
 from asc_cpp_b200 import synthetic
-from asc_cpp_b200._abi import (PLAN_HAS_ROW_GROUPS, PLAN_ROW_GROUPS, SPMM_STAGED, Determinism,
-                               SparseBlasTranspose)
-from asc_cpp_b200.sparse_cuda import CsrPlan, CudaSpmm, DenseMatrixView
+from asc_cpp_b200._abi import (PLAN_HAS_ROW_GROUPS, PLAN_ROW_GROUPS, SPMM_AUTO, SPMM_STAGED,
+                               Determinism, SparseBlasTranspose)
+from asc_cpp_b200.sparse_cuda import AscError, CsrPlan, CudaSpmm, DenseMatrixView
 from oracle import CSR, OP_NONE, ROW_MAJOR
 
 from gpu_util import bits_equal, context, csr, dev, host
@@ -55,7 +55,11 @@ def test_row_groups_bit_exact_every_group_size(cuda_lib, restatement, dt, k):
         a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
         plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
         got = spmm(ctx, plan, a, b, c0, -1.25, k)
-        assert bits_equal(got, want), (name, "default groups")
+        assert bits_equal(got, want), (name, "plan defaults")
+        for r in (2, 4, 8, 16, 32):  # every group size, chosen explicitly
+            plan.set_spmm(r)
+            assert plan.properties() & PLAN_HAS_ROW_GROUPS
+            assert bits_equal(spmm(ctx, plan, a, b, c0, -1.25, k), want), (name, r)
         # the autotuner's candidates, then the one it keeps
         scratch = dev(c0)
         ms, rg = plan.spmm_autotune(0.5, DenseMatrixView(dev(b), a_h.cols, k, writable=False),
@@ -76,6 +80,7 @@ def test_row_groups_default_mode_within_bound(cuda_lib, restatement, dt):
         c0 = rng.standard_normal((a_h.rows, k)).astype(dt)
         a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
         plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+        plan.set_spmm(8)
         got = spmm(ctx, plan, a, b, c0, 0.75, k)
         counts = np.diff(a_h.ptr)
         for j in range(k):
@@ -90,13 +95,15 @@ def test_row_groups_default_mode_within_bound(cuda_lib, restatement, dt):
     ctx.close()
 
 
-def test_stencil_groups_are_used(cuda_lib):
-    """A 27-point stencil shares most columns between neighbouring rows: the
-    plan keeps its groups (more than 1.25 entries per run)."""
+def test_groups_only_when_chosen(cuda_lib):
+    """Row groups run only when chosen (set_spmm or the autotuner); a plan
+    starts on its default kernels, and SPMM_AUTO returns to them."""
     a_h = synthetic.stencil_27(16, seed=2, dtype=np.float32)
     ctx = context()
     a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
     plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+    assert not plan.properties() & PLAN_HAS_ROW_GROUPS
+    plan.set_spmm(8)
     assert plan.properties() & PLAN_HAS_ROW_GROUPS
     b = np.random.default_rng(1).standard_normal((a_h.cols, 8)).astype(np.float32)
     c0 = np.zeros((a_h.rows, 8), np.float32)
@@ -105,5 +112,9 @@ def test_stencil_groups_are_used(cuda_lib):
     oracle.Restatement().standard_spmm(CSR, OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
                                        a_h.val, 1.0, b, ROW_MAJOR, 8, want, ROW_MAJOR, 8, 8)
     assert bits_equal(got, want)
+    plan.set_spmm(SPMM_AUTO)
+    assert not plan.properties() & PLAN_HAS_ROW_GROUPS
+    with pytest.raises(AscError):
+        plan.set_spmm(3)
     plan.close()
     ctx.close()

@@ -87,6 +87,7 @@ def test_staged_bit_exact(cuda_lib, restatement, dt, k):
         a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
         plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
         assert plan.properties() & PLAN_HAS_STAGED_SPMM, name
+        plan.set_spmm(SPMM_STAGED)  # at every k, not only the default range
         b = rng.standard_normal((a_h.cols, k)).astype(dt)
         c0 = rng.standard_normal((a_h.rows, k)).astype(dt)
         want = reference(restatement, a_h, b, c0, -1.25)
@@ -106,6 +107,7 @@ def test_staged_padded_leading_dimensions(cuda_lib, restatement, dt):
     for name, a_h in staged_shapes(rng, dt):
         a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
         plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+        plan.set_spmm(SPMM_STAGED)
         b = rng.standard_normal((a_h.cols, k)).astype(dt)
         c0 = rng.standard_normal((a_h.rows, k)).astype(dt)
         want = reference(restatement, a_h, b, c0, 0.5)
@@ -123,6 +125,7 @@ def test_staged_default_mode_within_bound(cuda_lib, restatement, dt):
     for name, a_h in staged_shapes(rng, dt):
         a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
         plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+        plan.set_spmm(SPMM_STAGED)
         b = rng.standard_normal((a_h.cols, k)).astype(dt)
         c0 = rng.standard_normal((a_h.rows, k)).astype(dt)
         got = run(ctx, plan, a, b, c0, 0.75)
@@ -182,6 +185,7 @@ def test_stages_beyond_shared_memory_fall_back(cuda_lib, restatement):
     a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
     plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
     assert plan.properties() & PLAN_HAS_STAGED_SPMM
+    plan.set_spmm(SPMM_STAGED)
     for k in (4, 128):
         b = rng.standard_normal((cols, k)).astype(np.float32)
         c0 = rng.standard_normal((n, k)).astype(np.float32)
