@@ -57,9 +57,12 @@ __host__ __device__ constexpr int64_t tile_items() {
 constexpr int kPer = 8;            // contiguous positions per lane
 constexpr int kChunk = 32;         // tile bounds cached per warp
 constexpr int kMaxDevices = 64;
-#ifndef ASCB_SEG_MIN_CTAS
-#define ASCB_SEG_MIN_CTAS 6
-#endif
+// CTAs per SM the segmented kernels are compiled for (register cap): on the
+// 4M-row power-law matrix (B200) the contracted tile runs best at 7 (72
+// registers: 2621 / 2667 GB/s plain / row split, against 2567 / 2524 at 6),
+// the bit-exact tile at 6 (2147 against 2022 GB/s at 7).
+constexpr int kMinCtasFast = 7;
+constexpr int kMinCtasExact = 6;
 
 // Row split (BACKEND_DEFAULT): a tile whose last row runs more than
 // `split_min` positions past the tile's window does not walk that tail
@@ -582,7 +585,7 @@ __device__ __forceinline__ void seg_tile(SegSmem<T>& w, int lane, const int64_t*
 
 template <typename T, bool EXACT, bool STANDARD, bool UNIT, bool SPLIT = false, bool V32 = false,
           int RPL = 1>
-__global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
+__global__ void __launch_bounds__(kThreads, EXACT ? kMinCtasExact : kMinCtasFast)
 seg_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ idx,
            const T* __restrict__ val, const T* __restrict__ x, int64_t incx, T* __restrict__ y,
            int64_t incy, T alpha, T beta, const int64_t* __restrict__ tile_row, int64_t ntiles,
@@ -753,7 +756,7 @@ __global__ void batch_bounds_kernel(const ascb_batch_item* __restrict__ items, i
 }
 
 template <typename T, bool EXACT, bool UNIT>
-__global__ void __launch_bounds__(kThreads, ASCB_SEG_MIN_CTAS)
+__global__ void __launch_bounds__(kThreads, EXACT ? kMinCtasExact : kMinCtasFast)
 seg_batch_kernel(const ascb_batch_item* __restrict__ items, int64_t count,
                  const int64_t* __restrict__ bounds, int64_t total_tiles,
                  unsigned long long* __restrict__ queue, int chunk, T alpha, T beta) {
