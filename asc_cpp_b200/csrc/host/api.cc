@@ -171,8 +171,10 @@ int Finish(asc_sb_context* ctx, const Status& s) {
 
 // Launch result -> status; after a failed enqueue the stream is drained so the
 // caller can release operands safely (operations.cc:1027-1045).
-Status Launched(asc_sb_context* ctx, int err, const char* message) {
-  ctx->launches.fetch_add(1, std::memory_order_relaxed);
+// Result of an enqueue of `kernels` kernels (counted in the context's launch
+// counter).
+Status Launched(asc_sb_context* ctx, int err, const char* message, int kernels = 1) {
+  ctx->launches.fetch_add(kernels, std::memory_order_relaxed);
   if (err == 0) return Status::Ok();
   (void)cudaStreamSynchronize(ctx->stream);
   (void)cudaGetLastError();
@@ -369,7 +371,7 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
                       ascb_spmv_split(ctx->stream, dtype, form, &a, alpha, beta, &x, &y,
                                       tiles_ptr, tiles, weight, rounds * ascb_warp_tile_items(),
                                       block, ctx->sm_count),
-                      "CUDA could not launch the row-split SpMV kernels");
+                      "CUDA could not launch the row-split SpMV kernels", 2);
     }
   }
   if (seg_aligned) {
@@ -1261,7 +1263,7 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
                                          c->leading_dimension, static_cast<float>(alpha_real),
                                          reinterpret_cast<float*>(tiles), ctx->status,
                                          ctx->sm_count),
-                    "CUDA could not launch the tensor-core SpMM kernel");
+                    "CUDA could not launch the tensor-core SpMM kernel", 2);
   }
   if (!RealKind(m->element_kind)) {
     const int mode = transposed && !planned ? 2 : (ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0);

@@ -327,7 +327,8 @@ def selector_leg(count=40, seed=5, max_rows=1_000_000, reps=10):
     (training used seed 4), each multiplied through CudaCsrSpmv (the C ABI
     entry a reference caller reaches) in BACKEND_DEFAULT mode with the shipped
     selector installed (the context's default), against the default variant
-    forced and against exhaustive autotuning (every candidate timed)."""
+    forced and against exhaustive search on the same path (every candidate
+    forced through CudaCsrSpmv and timed)."""
     import ctypes
     import torch
     from asc_cpp_b200 import selector as sel
@@ -367,15 +368,14 @@ def selector_leg(count=40, seed=5, max_rows=1_000_000, reps=10):
         plan = sc.CsrPlan(ctx, m)  # the same selector on a plan: which variant it is
         v, l = ctypes.c_int32(), ctypes.c_int32()
         ctx.check(ctx._lib.asc_sb_plan_variant(plan.handle, ctypes.byref(v), ctypes.byref(l)))
-        ms = np.zeros(len(variants), np.float32)
-        xd, yd = xv.describe(), yv.describe()
-        xd.writable = 0
-        ctx.check(ctx._lib.asc_sb_plan_autotune(ctx.handle, plan.handle, ctypes.byref(xd),
-                                                ctypes.byref(yd), len(variants),
-                                                variants.ctypes.data, lanes.ctypes.data, reps,
-                                                ms.ctypes.data))
         plan.close()
-        rows.append((family, m.rows, m.nnz, t_default, t_pick, float(ms.min()),
+        # exhaustive on the same path: every candidate forced through CudaCsrSpmv
+        forced = []
+        for vv, ll in zip(variants, lanes):
+            ctx.set_variant(int(vv), int(ll))
+            forced.append(timed(product))
+        ctx.set_variant(Variant.kAuto, 0)
+        rows.append((family, m.rows, m.nnz, t_default, t_pick, float(min(forced)),
                      (int(v.value), int(l.value))))
         del m, x, y, ws
     ctx.close()
