@@ -25,9 +25,10 @@
 //
 // B tiles: a pre-pass (bt_tiles_kernel, once per product) writes, for every
 // block column and 128-column chunk of B, the two 8 KB shared-memory images
-// hi and lo of B_blk^T (zero rows past k), so a stage's B operand arrives as
-// ONE 16 KB TMA bulk copy (cp.async.bulk) from L2 -- no transposes, splits or
-// LSU traffic for B in the main kernel.
+// hi and lo of B_blk^T, so a stage's B operand arrives as two TMA bulk copies
+// (cp.async.bulk) of the chunk's `width` rows (16 KB at 128 right-hand sides,
+// 1 KB at 8) from L2 -- no transposes, splits or LSU traffic for B in the
+// main kernel.
 //
 // Pipeline: four producer warps each own one shared-memory stage and fill it
 // for the blocks whose running index is their warp number mod 4: lane 0
@@ -172,11 +173,12 @@ bt_tiles_kernel(const float* __restrict__ b, int64_t ldb, int64_t k, int64_t b_r
     const int64_t tile = i / (kM * 4);  // bc * chunks + ch
     const int64_t bc = tile / chunks;
     const int64_t col = (tile - bc * chunks) * kM + m;
+    if (col >= k) continue;  // rows past k are never copied (see the producers)
     float v[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int64_t row = bc * kB + cq * 4 + e;
-      v[e] = col < k && row < b_rows ? __ldg(b + row * ldb + col) : 0.0f;
+      v[e] = row < b_rows ? __ldg(b + row * ldb + col) : 0.0f;
     }
     float4 hi, lo;
     split(make_float4(v[0], v[1], v[2], v[3]), hi, lo);
@@ -294,10 +296,15 @@ block16_tc_kernel(const int64_t* __restrict__ ptr, const int64_t* __restrict__ i
           break;
         }
         if (lane == 0) {
-          // B^T hi and lo of (bc, ch): one bulk copy into the stage
-          mbar_expect_tx(&s.full[p], 2 * kTileFloats * 4);
-          bulk_copy(bt_hi, tiles + (bc * chunks + ch) * 2 * kTileFloats, 2 * kTileFloats * 4,
-                    &s.full[p]);
+          // rows [0, width) of B^T hi and lo of (bc, ch): a row is 64 bytes and
+          // the swizzle permutes chunks only within a row, so the images'
+          // first `width` rows are contiguous.  Rows past width keep stale data:
+          // they feed only rows of D past width, which the epilogue never stores.
+          const uint32_t bytes = static_cast<uint32_t>(width) * kB * 4;
+          const float* src = tiles + (bc * chunks + ch) * 2 * kTileFloats;
+          mbar_expect_tx(&s.full[p], 2 * bytes);
+          bulk_copy(bt_hi, src, bytes, &s.full[p]);
+          bulk_copy(bt_hi + kTileFloats * 4, src + kTileFloats, bytes, &s.full[p]);
         }
         float4 hi, lo;
         split(va0, hi, lo);

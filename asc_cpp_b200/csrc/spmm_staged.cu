@@ -393,14 +393,16 @@ spmm_staged_kernel(StagedArgs a, T alpha) {
       const auto* sptr = reinterpret_cast<const int64_t*>(base + a.lay.ptr) + hdr->lead_p;
       const auto* sval = reinterpret_cast<const T*>(base + a.lay.val) + hdr->lead_v;
       const auto* sslot = reinterpret_cast<const uint16_t*>(base + a.lay.slot) + hdr->lead_s;
-      const V* sb = reinterpret_cast<const V*>(base + a.lay.b);
+      // 32-bit shared-memory byte offsets: this lane's first chunk of slot 0
+      const uint32_t rbytes = static_cast<uint32_t>(row_bytes);
+      const unsigned char* sbb = base + a.lay.b + static_cast<uint32_t>(lc) * 16u;
       for (int rl = tid / G; rl < nrows; rl += kThreads / G) {
-        const int64_t o = r0 + rl;
-        const int64_t pb = sptr[rl] - z0;
-        const int64_t pe = sptr[rl + 1] - z0;
+        const int pb = static_cast<int>(sptr[rl] - z0);
+        const int pe = static_cast<int>(sptr[rl + 1] - z0);
         if (pb == pe) continue;  // C unchanged in both forms
-        const int64_t soff = hdr->slots[rl / kGroupRows] - slot0;
-        T* crow = cmat + o * a.ldc;
+        const unsigned char* rowb =
+            sbb + static_cast<uint32_t>(hdr->slots[rl / kGroupRows] - slot0) * rbytes;
+        T* crow = cmat + (r0 + rl) * a.ldc;
         T acc[J][N];
         bool live[J];
 #pragma unroll
@@ -414,20 +416,22 @@ spmm_staged_kernel(StagedArgs a, T alpha) {
             for (int e = 0; e < N; ++e) acc[t][e] = T(0);
           }
         }
-        int64_t q = pb;
+        int q = pb;
         for (; q + kUnroll <= pe; q += kUnroll) {
           T av[kUnroll];
-          int64_t sl[kUnroll];
+          uint32_t sl[kUnroll];
 #pragma unroll
           for (int u = 0; u < kUnroll; ++u) {
             av[u] = EXACT ? mul_rn(alpha, sval[q + u]) : sval[q + u];
-            sl[u] = (soff + sslot[q + u]) * a.chunks;
+            sl[u] = static_cast<uint32_t>(sslot[q + u]) * rbytes;
           }
           V bv[kUnroll][J];
 #pragma unroll
           for (int u = 0; u < kUnroll; ++u) {
 #pragma unroll
-            for (int t = 0; t < J; ++t) bv[u][t] = live[t] ? sb[sl[u] + lc + t * G] : V{};
+            for (int t = 0; t < J; ++t) {
+              bv[u][t] = live[t] ? *reinterpret_cast<const V*>(rowb + sl[u] + t * G * 16) : V{};
+            }
           }
 #pragma unroll
           for (int u = 0; u < kUnroll; ++u) {
@@ -445,12 +449,12 @@ spmm_staged_kernel(StagedArgs a, T alpha) {
         }
         for (; q < pe; ++q) {
           const T av = EXACT ? mul_rn(alpha, sval[q]) : sval[q];
-          const int64_t sl = (soff + sslot[q]) * a.chunks;
+          const uint32_t sl = static_cast<uint32_t>(sslot[q]) * rbytes;
 #pragma unroll
           for (int t = 0; t < J; ++t) {
             if (!live[t]) continue;
             T e[N];
-            W::split(sb[sl + lc + t * G], e);
+            W::split(*reinterpret_cast<const V*>(rowb + sl + t * G * 16), e);
 #pragma unroll
             for (int k = 0; k < N; ++k) {
               acc[t][k] = EXACT ? add_rn(acc[t][k], mul_rn(av, e[k])) : fma(av, e[k], acc[t][k]);
