@@ -60,7 +60,7 @@ constexpr int kMaxDevices = 64;
 // CTAs per SM the segmented kernels are compiled for (register cap): on the
 // 4M-row power-law matrix (B200) the contracted tile runs best at 7 (72
 // registers: 2621 / 2667 GB/s plain / row split, against 2567 / 2524 at 6),
-// the bit-exact tile at 6 (2147 against 2022 GB/s at 7).
+// the bit-exact tile at 6 (2250 against 2168 GB/s at 7, and 1895 at 5).
 constexpr int kMinCtasFast = 7;
 constexpr int kMinCtasExact = 6;
 
@@ -230,19 +230,21 @@ __device__ __forceinline__ void lane_products(T (&p)[kPer], uint32_t vmask,
   }
 }
 
-// A lane's 8 products into its 8 consecutive shared-memory slots without bank
-// conflicts.  Lane l owns bytes [8 l sizeof(T), ...): stored chunk by chunk in
-// the same order by every lane, every second (FP64) or fourth (FP32) lane
-// hits the same banks.  Lane l stores its 16-byte chunk (j + l / 2) % 4 in step
-// j instead (FP32: (j + l / 4) % 2), so 8 consecutive lanes cover all 32 banks.
+// A lane's 8 products into its 8 consecutive shared-memory slots.  Lane l
+// owns bytes [8 l sizeof(T), ...): stored chunk by chunk in the same order by
+// every lane, every second (FP64) or fourth (FP32) lane hits the same banks.
+// FP64: lane l stores its 16-byte chunk j ^ ((l / 2) & 1) in step j, so each
+// 16-byte store meets at most 2-way conflicts for 16 selects per lane (the
+// conflict-free rotation (j + l / 2) % 4 needs 48 and measured 2.3% slower on
+// the 4M-row power-law matrix).  FP32: chunk (j + l / 4) % 2, conflict-free.
 __device__ __forceinline__ void store_run(double* dst, int lane, const double (&p)[kPer]) {
-  const int h = (lane >> 1) & 3;
+  const bool h = ((lane >> 1) & 1) != 0;
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
-    const int c = (j + h) & 3;
-    double2 v;  // chunk c of p, selected without dynamic register indexing
-    v.x = c == 0 ? p[0] : c == 1 ? p[2] : c == 2 ? p[4] : p[6];
-    v.y = c == 0 ? p[1] : c == 1 ? p[3] : c == 2 ? p[5] : p[7];
+    const int c = j ^ (h ? 1 : 0);
+    double2 v;
+    v.x = h ? p[2 * (j ^ 1)] : p[2 * j];
+    v.y = h ? p[2 * (j ^ 1) + 1] : p[2 * j + 1];
     *reinterpret_cast<double2*>(dst + 2 * c) = v;
   }
 }
@@ -252,6 +254,34 @@ __device__ __forceinline__ void store_run(float* dst, int lane, const float (&p)
   const float4 hi = make_float4(p[4], p[5], p[6], p[7]);
   *reinterpret_cast<float4*>(dst + (h ? 4 : 0)) = h ? hi : lo;
   *reinterpret_cast<float4*>(dst + (h ? 0 : 4)) = h ? lo : hi;
+}
+
+// acc + prod[q] + prod[q + 1] + ... + prod[e - 1], each sum rounded, in that
+// order; the aligned middle is read with 16-byte shared loads (prod is
+// 16-byte aligned).
+__device__ __forceinline__ double chain_sum(double acc, const double* prod, int q, int e) {
+  if ((q & 1) && q < e) acc = add_rn(acc, prod[q++]);
+  for (; q + 4 <= e; q += 4) {
+    const double2 u = *reinterpret_cast<const double2*>(prod + q);
+    const double2 v = *reinterpret_cast<const double2*>(prod + q + 2);
+    acc = add_rn(add_rn(add_rn(add_rn(acc, u.x), u.y), v.x), v.y);
+  }
+  if (q + 2 <= e) {
+    const double2 u = *reinterpret_cast<const double2*>(prod + q);
+    acc = add_rn(add_rn(acc, u.x), u.y);
+    q += 2;
+  }
+  if (q < e) acc = add_rn(acc, prod[q]);
+  return acc;
+}
+__device__ __forceinline__ float chain_sum(float acc, const float* prod, int q, int e) {
+  for (; (q & 3) && q < e; ++q) acc = add_rn(acc, prod[q]);
+  for (; q + 4 <= e; q += 4) {
+    const float4 u = *reinterpret_cast<const float4*>(prod + q);
+    acc = add_rn(add_rn(add_rn(add_rn(acc, u.x), u.y), u.z), u.w);
+  }
+  for (; q < e; ++q) acc = add_rn(acc, prod[q]);
+  return acc;
 }
 
 // EXACT tile: the window's products are formed in parallel (8 contiguous
@@ -307,12 +337,7 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
     T racc = STANDARD ? *rp : T(0);
     const int s0 = static_cast<int>(b - a0);
     const int e0 = static_cast<int>(e - a0 < lim ? e - a0 : lim);
-    int q = s0;
-    for (; q + 4 <= e0; q += 4) {
-      const T u0 = w.prod[q], u1 = w.prod[q + 1], u2 = w.prod[q + 2], u3 = w.prod[q + 3];
-      racc = add_rn(add_rn(add_rn(add_rn(racc, u0), u1), u2), u3);
-    }
-    for (; q < e0; ++q) racc = add_rn(racc, w.prod[q]);
+    racc = chain_sum(racc, w.prod, s0, e0);
     if (carries && k == nr - 1) {
       acc = racc;
       yp = rp;
@@ -333,14 +358,7 @@ __device__ __forceinline__ void exact_tile(SegSmem<T>& w, int lane,
                                                   val + (q0 + p0), x, incx, alpha);
       store_run(w.prod + p0, lane, q);
       __syncwarp();
-      if (carries) {
-        int k = 0;
-        for (; k + 4 <= cnt; k += 4) {
-          const T u0 = w.prod[k], u1 = w.prod[k + 1], u2 = w.prod[k + 2], u3 = w.prod[k + 3];
-          acc = add_rn(add_rn(add_rn(add_rn(acc, u0), u1), u2), u3);
-        }
-        for (; k < cnt; ++k) acc = add_rn(acc, w.prod[k]);
-      }
+      if (carries) acc = chain_sum(acc, w.prod, 0, cnt);
     }
     if (carries) *yp = finish<true, STANDARD>(acc, alpha, beta, yp);
   }
