@@ -219,6 +219,8 @@ SIGNATURES: dict[str, tuple] = {
                                                  ctypes.POINTER(ctypes.c_float),
                                                  ctypes.POINTER(_I32)]),
     "asc_sb_plan_set_spmm": (ctypes.c_int, [_P, _P, _I32]),
+    "asc_sb_plan_spmm_stage_rows": (ctypes.c_int, [_P, _P, ctypes.c_int64,
+                                                   ctypes.POINTER(ctypes.c_int64)]),
     "asc_sb_plan_spmm_tuning": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_I32),
                                                ctypes.POINTER(_I32),
                                                ctypes.POINTER(ctypes.c_float)]),

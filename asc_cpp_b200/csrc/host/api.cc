@@ -121,15 +121,17 @@ struct asc_sb_plan {
   std::int64_t group_run_count = 0;
   bool use_groups = false;  // SpMM through the groups (reuse measured or tuned)
   // ASC_SB_PLAN_ROW_GROUPS also builds the TMA-staged SpMM tables (groups of
-  // 16 rows); caps[2w], caps[2w + 1]: largest slot and entry counts of a
-  // stage of 2^w groups
+  // 16 rows, and wide groups of 32 and 64 whose shared columns are one slot);
+  // staged_caps[v][2w], [2w + 1]: largest slot and entry counts of a stage
+  // of 2^w groups of level v
   unsigned char* staged_mem = nullptr;
-  ascb_staged_spmm staged{};
-  std::int64_t staged_caps[10] = {};
+  ascb_staged_spmm staged[ASCB_STAGED_LEVELS] = {};
+  std::int64_t staged_caps[ASCB_STAGED_LEVELS][10] = {};
+  bool level_ok[ASCB_STAGED_LEVELS] = {};  // no group of the level exceeds 65534 slots
   std::int64_t staged_slots = 0;  // distinct columns over all 16-row groups
   bool has_staged = false;
   bool use_staged = false;    // SpMM through the staged kernel where it fits ...
-  bool staged_tuned = false;  // ... for every k (the autotuner picked it), else for 16 <= k <= 64
+  bool staged_tuned = false;  // ... for every k (the autotuner picked it), else for k >= 8
   // the last SpMM autotune: candidates timed and their ms per product
   int tuned_count = 0;
   int tuned_candidate[8] = {};
@@ -516,19 +518,25 @@ Status BuildStaged(asc_sb_context* ctx, asc_sb_plan* plan) {
   const int elem = static_cast<int>(ascb::host::ElementBytes(plan->matrix.element_kind));
   Status s = Launched(ctx,
                       ascb_staged_build(ctx->stream, &a, &plan->groups, plan->groups_mem, elem,
-                                        plan->staged_mem, &plan->staged, ctx->sm_count),
+                                        plan->staged_mem, plan->staged, ctx->sm_count),
                       "CUDA could not launch the staged SpMM build");
   if (!s.ok()) return s;
-  unsigned long long caps[10] = {};
-  cudaError_t e = cudaMemcpyAsync(caps, plan->staged.caps, sizeof(caps), cudaMemcpyDeviceToHost,
-                                  ctx->stream);
+  unsigned long long caps[ASCB_STAGED_LEVELS][10] = {};
+  cudaError_t e = cudaSuccess;
+  for (int v = 0; v < ASCB_STAGED_LEVELS && e == cudaSuccess; ++v) {
+    e = cudaMemcpyAsync(caps[v], plan->staged[v].caps, sizeof(caps[v]), cudaMemcpyDeviceToHost,
+                        ctx->stream);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     (void)cudaGetLastError();
     return {ASC_SB_PROVIDER, std::string("CUDA could not build the staged SpMM tables: ") +
                                  cudaGetErrorString(e)};
   }
-  for (int i = 0; i < 10; ++i) plan->staged_caps[i] = static_cast<std::int64_t>(caps[i]);
+  for (int v = 0; v < ASCB_STAGED_LEVELS; ++v) {
+    for (int i = 0; i < 10; ++i) plan->staged_caps[v][i] = static_cast<std::int64_t>(caps[v][i]);
+    plan->level_ok[v] = plan->staged_caps[v][0] < 65535;
+  }
   plan->has_staged = true;
   const std::int64_t slots = plan->group_run_count;  // of the 16-row groups
   plan->staged_slots = slots;
@@ -1173,29 +1181,51 @@ bool GroupsApply(const asc_sb_dense& b, const asc_sb_dense& c, int kind) {
 }
 
 // The staged kernel's operand rules (those of the row groups) and the room
-// it needs: two stages of the plan's largest stage for this k in one CTA's
-// shared memory.  *ng, *slots, *entries: the stage width and its caps.
+// it needs: two stages of the level's largest stage for this k in one CTA's
+// shared memory.  Of the levels that fit, the one that keeps the most CTAs
+// per SM, the widest groups (fewest bulk copies) among equals: on a 27-point
+// 128^3 stencil (FP32, B200) wide groups of 64 rows take k = 8 from 0.54 to
+// 0.28 ms, but at k = 32 their 87 KB stages leave one CTA per SM (0.76 ms
+// against 0.61 for the 16-row groups' two).  *level: the tables to run;
+// *slots, *entries: the stage's caps.
 bool StagedApply(const asc_sb_plan& plan, const asc_sb_dense& b, const asc_sb_dense& c, int kind,
-                 int device, std::int64_t* slots, std::int64_t* entries) {
+                 int device, const ascb_staged_spmm** level, std::int64_t* slots,
+                 std::int64_t* entries) {
   if (!plan.has_staged || !GroupsApply(b, c, kind)) return false;
   const int dtype = Dtype(kind);
   // at most 128 chunks of 16 bytes per row (32 lanes x 4 chunks)
   if (c.columns * static_cast<std::int64_t>(ascb::host::ElementBytes(kind)) > 128 * 16) {
     return false;
   }
-  const int ng = ascb_staged_groups_per_stage(dtype, c.columns);
-  int w = 0;
-  while ((1 << w) < ng) ++w;
-  *slots = plan.staged_caps[2 * w];
-  *entries = plan.staged_caps[2 * w + 1];
-  int optin = 0;
+  int optin = 0, per_sm = 0;
   if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) !=
-      cudaSuccess) {
+          cudaSuccess ||
+      cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, device) !=
+          cudaSuccess) {
     (void)cudaGetLastError();
     return false;
   }
-  const std::size_t stage = ascb_staged_stage_bytes(dtype, c.columns, *slots, *entries, ng);
-  return 2 * stage <= static_cast<std::size_t>(optin);
+  std::int64_t best_ctas = 0;
+  for (int v = ASCB_STAGED_LEVELS - 1; v >= 0; --v) {
+    if (!plan.level_ok[v]) continue;
+    const ascb_staged_spmm& t = plan.staged[v];
+    const std::int64_t* caps = plan.staged_caps[v];
+    const int ng = ascb_staged_groups_per_stage(dtype, c.columns, t.group_rows);
+    int w = 0;
+    while ((1 << w) < ng) ++w;
+    const std::size_t stage =
+        ascb_staged_stage_bytes(dtype, c.columns, caps[2 * w], caps[2 * w + 1], ng, t.group_rows);
+    if (2 * stage > static_cast<std::size_t>(optin)) continue;
+    // CTAs per SM by shared memory (1 KB reserved per CTA)
+    const std::int64_t ctas =
+        std::max<std::int64_t>(1, per_sm / static_cast<std::int64_t>(2 * stage + 1024));
+    if (ctas <= best_ctas) continue;
+    best_ctas = ctas;
+    *level = &t;
+    *slots = caps[2 * w];
+    *entries = caps[2 * w + 1];
+  }
+  return best_ctas > 0;
 }
 
 // C += alpha * op(A) * B, validated in full before anything is enqueued.  With
@@ -1276,20 +1306,22 @@ Status StandardSpmm(asc_sb_context* ctx, const asc_sb_plan* plan, int op, double
                                       ctx->sm_count),
                     "CUDA could not launch the complex SpMM kernel");
   }
-  // the staged kernel by default for 16 <= k <= 64 elements (on a 27-point
-  // 128^3 stencil, B200: k = 32 0.60 ms against 0.62 ms contracted and 0.62
-  // against 0.87 ms bit-exact; k = 8 0.54 against 0.31 ms -- B rows of 32
-  // bytes make the bulk copies too small; k = 128 3.1 against 1.75 ms --
-  // shared-memory reads bound it); for any k once the autotuner picked it
+  // the staged kernel by default for k >= 8 elements where its stages fit
+  // (27-point 128^3 stencil, FP32, B200, contracted / bit-exact: k = 8 0.25 /
+  // 0.26 ms against 0.31 / 0.30 row by row, k = 32 0.49 / 0.53 against 0.62 /
+  // 0.86, k = 128 2.09 / 2.25 against 2.32 / 2.50); for any k once the
+  // autotuner picked it
   std::int64_t st_slots = 0, st_entries = 0;
-  const bool staged_k = c->columns >= 16 && c->columns <= 64;
+  const ascb_staged_spmm* st_level = nullptr;
+  const bool staged_k = c->columns >= 8;
   if (!transposed && !csc && plan != nullptr && plan->use_staged &&
       (plan->staged_tuned || staged_k) &&
-      StagedApply(*plan, *b, *c, m->element_kind, ctx->device, &st_slots, &st_entries)) {
+      StagedApply(*plan, *b, *c, m->element_kind, ctx->device, &st_level, &st_slots,
+                  &st_entries)) {
     return Launched(ctx,
                     ascb_spmm_staged(ctx->stream, Dtype(m->element_kind),
                                      ctx->determinism == ASC_SB_DETERMINISTIC ? 1 : 0, &a,
-                                     &plan->staged, c->columns, b->data, b->leading_dimension,
+                                     st_level, c->columns, b->data, b->leading_dimension,
                                      const_cast<void*>(c->data), c->leading_dimension,
                                      alpha_real, st_slots, st_entries, ctx->status,
                                      ctx->sm_count),
@@ -2098,8 +2130,9 @@ int asc_sb_plan_spmm_autotune(asc_sb_context* ctx, asc_sb_plan* plan, double alp
   // TMA-staged kernel, else R rows per group
   const int candidates[] = {0, ASC_SB_SPMM_STAGED, 2, 4, 8, 16, 32};
   std::int64_t st_slots = 0, st_entries = 0;
-  const bool staged_ok =
-      StagedApply(*plan, *b, *c, plan->matrix.element_kind, ctx->device, &st_slots, &st_entries);
+  const ascb_staged_spmm* st_level = nullptr;
+  const bool staged_ok = StagedApply(*plan, *b, *c, plan->matrix.element_kind, ctx->device,
+                                     &st_level, &st_slots, &st_entries);
   plan->tuned_count = 0;
   cudaEvent_t start = nullptr, stop = nullptr;
   cudaError_t e = cudaEventCreate(&start);
@@ -2178,6 +2211,28 @@ int asc_sb_plan_set_spmm(asc_sb_context* ctx, asc_sb_plan* plan, int32_t choice)
                      (choice == ASC_SB_SPMM_AUTO && plan->has_staged &&
                       4 * plan->matrix.nonzeros >= 5 * plan->staged_slots);
   plan->staged_tuned = choice == ASC_SB_SPMM_STAGED;
+  return Finish(ctx, Status::Ok());
+}
+
+int asc_sb_plan_spmm_stage_rows(asc_sb_context* ctx, const asc_sb_plan* plan, int64_t k,
+                                int64_t* rows) {
+  Status s = ValidateContext(ctx);
+  if (!s.ok()) return Finish(ctx, s);
+  if (plan == nullptr || rows == nullptr || k < 0) {
+    return Finish(ctx, Fail(ASC_SB_INVALID_ARGUMENT, "stage-rows arguments are invalid"));
+  }
+  *rows = 0;
+  asc_sb_dense b{}, c{};
+  b.layout = c.layout = ASC_SB_ROW_MAJOR;
+  b.element_kind = c.element_kind = plan->matrix.element_kind;
+  b.columns = c.columns = k;
+  b.leading_dimension = c.leading_dimension = k;
+  const ascb_staged_spmm* level = nullptr;
+  std::int64_t slots = 0, entries = 0;
+  if (k > 0 && StagedApply(*plan, b, c, plan->matrix.element_kind, ctx->device, &level, &slots,
+                           &entries)) {
+    *rows = level->group_rows;
+  }
   return Finish(ctx, Status::Ok());
 }
 

@@ -277,12 +277,15 @@ int ascb_spmm_groups(void* stream, int dtype, int exact, const ascb_csr* a,
 // i <= n (out holds n + 1); `sums`: (n / 2048 + 2) int64 of scratch.
 int ascb_scan_i64(void* stream, const int64_t* in, int64_t n, int64_t* out, int64_t* sums);
 
-// ---- TMA-staged SpMM (plan-built groups of 16 rows) ----
-// Per group of 16 rows: its distinct columns ("slots", column order), their
+// ---- TMA-staged SpMM (plan-built groups of 16, 32 and 64 rows) ----
+// Per group of rows: its distinct columns ("slots", column order), their
 // maximal runs of consecutive columns ("segments"), and per stored entry the
-// slot of its column.
+// slot of its column.  Three levels: groups of 16 rows, and wide groups of 32
+// and 64 (two or four groups merged: a column they share is one slot).
+#define ASCB_STAGED_LEVELS 3
 typedef struct ascb_staged_spmm {
   int64_t groups;
+  int64_t group_rows;   // 16, 32 or 64
   int64_t* group_runs;  // [groups + 1] slots before each group
   int64_t* group_segs;  // [groups + 1] segments before each group
   int64_t* seg_col;     // [segments] first column
@@ -293,27 +296,34 @@ typedef struct ascb_staged_spmm {
   // 1, 2, 4, 8, 16 groups (pairs, in that order)
   unsigned long long* caps;
 } ascb_staged_spmm;
+typedef struct ascb_staged_level_layout {
+  size_t group_runs, group_segs, seg_col, seg_run, seg_len, slot, caps;
+} ascb_staged_level_layout;
 typedef struct ascb_staged_layout {
-  size_t group_runs, group_segs, seg_col, seg_run, seg_len, slot, caps, persistent;
-  size_t seg_flag, seg_of, sums, total;
+  ascb_staged_level_layout level[ASCB_STAGED_LEVELS];  // 16, 32, 64 rows
+  size_t persistent;
+  size_t seg_flag, seg_of, sums, wide_slot_of, wide_col, total;
 } ascb_staged_layout;
 // Byte offsets in a 256-byte aligned block; [persistent, total) is build
 // scratch.
 ascb_staged_layout ascb_staged_layout_for(int64_t rows, int64_t nnz);
-// Builds the staged tables from row groups of 16 rows just built by
+// Builds every level's tables (levels[0 .. ASCB_STAGED_LEVELS): groups of
+// 16, 32, 64 rows) from row groups of 16 rows just built by
 // ascb_row_groups_build into `groups_base` (it reads that build's scratch).
 int ascb_staged_build(void* stream, const ascb_csr* a, const ascb_row_groups* rg16,
                       const void* groups_base, int elem_bytes, void* base,
-                      ascb_staged_spmm* out, int sm_count);
-// Groups per pipeline stage for k right-hand sides, and the bytes of one
-// stage holding `slots` rows of B and `entries` stored entries.
-int ascb_staged_groups_per_stage(int dtype, int64_t k);
-size_t ascb_staged_stage_bytes(int dtype, int64_t k, int64_t slots, int64_t entries, int ng);
+                      ascb_staged_spmm* levels, int sm_count);
+// Groups per pipeline stage for k right-hand sides (a stage holds at least
+// the rows one pass of the consumers covers), and the bytes of one stage
+// holding `slots` rows of B and `entries` stored entries.
+int ascb_staged_groups_per_stage(int dtype, int64_t k, int64_t group_rows);
+size_t ascb_staged_stage_bytes(int dtype, int64_t k, int64_t slots, int64_t entries, int ng,
+                               int64_t group_rows);
 // C += alpha * A * B (row-major B and C, rows of whole 16-byte chunks on
-// 16-byte boundaries); max_slots / max_entries: the caps of the stage width
-// ascb_staged_groups_per_stage(dtype, k); exact = 1: the reference's
-// per-entry update in stored order (bit-exact).  Two stages of
-// ascb_staged_stage_bytes each must fit one CTA's shared memory.
+// 16-byte boundaries) over the groups of `st` (either level); max_slots /
+// max_entries: the caps of the stage width ascb_staged_groups_per_stage;
+// exact = 1: the reference's per-entry update in stored order (bit-exact).
+// Two stages of ascb_staged_stage_bytes each must fit one CTA's shared memory.
 int ascb_spmm_staged(void* stream, int dtype, int exact, const ascb_csr* a,
                      const ascb_staged_spmm* st, int64_t k, const void* b, int64_t ldb, void* c,
                      int64_t ldc, double alpha, int64_t max_slots, int64_t max_entries,

@@ -472,6 +472,14 @@ class CsrPlan:
         self.context.check(self.context._lib.asc_sb_plan_set_spmm(self.context.handle, self._h,
                                                                    int(choice)))
 
+    def spmm_stage_rows(self, k: int) -> int:
+        """Rows per group of the staged SpMM tables a product with k columns
+        (row-major, leading dimension k) would use: 16, 32, 64 or 0."""
+        rows = ctypes.c_int64()
+        self.context.check(self.context._lib.asc_sb_plan_spmm_stage_rows(
+            self.context.handle, self._h, int(k), ctypes.byref(rows)))
+        return int(rows.value)
+
     def spmm_tuning(self) -> dict[int, float]:
         """The last spmm_autotune's table: {candidate: ms per product}."""
         count = ctypes.c_int32()

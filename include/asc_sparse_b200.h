@@ -383,13 +383,15 @@ ASC_SB_API int asc_sb_clone_indexed(asc_sb_context* context,
 /* ASC_SB_PLAN_ROW_GROUPS (CSR, float or double) prepares two more SpMM
  * kernels for asc_sb_plan_standard_spmm with op = none and row-major B and C
  * whose rows are whole 16-byte chunks on 16-byte boundaries:
- *   - the TMA-staged kernel: per group of 16 rows, the distinct columns in
- *     runs of consecutive columns and per stored entry the slot of its
- *     column; a producer warp per CTA stages a group's rows of B, row
- *     offsets, values and slots in shared memory with bulk copies (two-stage
- *     pipeline) and the other warps compute from there.  By default it runs
- *     when the groups share columns (at least 1.25 entries per distinct
- *     column), 16 <= k <= 64 and two stages fit one CTA's shared memory;
+ *   - the TMA-staged kernel: per group of 16, 32 or 64 rows (three levels;
+ *     asc_sb_plan_spmm_stage_rows), the distinct columns in runs of
+ *     consecutive columns and per stored entry the slot of its column; a
+ *     producer warp per CTA stages a stage's rows of B, row offsets, values,
+ *     slots (and long rows of C) in shared memory with bulk copies
+ *     (two-stage pipeline) and the other warps compute from there.  By
+ *     default it runs when the groups share columns (at least 1.25 entries
+ *     per distinct column of a 16-row group), k >= 8 and two stages fit one
+ *     CTA's shared memory;
  *   - row groups of R rows (R = 8 at creation): runs -- one per distinct
  *     column, with the rows that hold it -- so that each row of B is loaded
  *     once per run and applied to all of the run's rows.  Used only when
@@ -463,6 +465,16 @@ ASC_SB_API int asc_sb_plan_spmm_autotune(asc_sb_context* context,
                                          const asc_sb_dense* input,
                                          const asc_sb_dense* output, int32_t reps,
                                          float* best_ms, int32_t* rows_per_group);
+/* Rows per group of the staged SpMM tables a product with k columns of
+ * row-major B and C (leading dimension k) would run on: 16, 32 or 64 (wide
+ * groups of two or four 16-row groups, one slot per distinct column) -- of
+ * the levels whose two stages fit a CTA's shared memory, the one that keeps
+ * the most CTAs per SM, the widest among equals -- or 0 where the staged
+ * kernel does not apply (no staged tables, element kind or k unsupported, or
+ * no stage fits).  Whether the staged kernel runs at all is the plan's SpMM
+ * choice (ASC_SB_PLAN_HAS_STAGED_SPMM, asc_sb_plan_set_spmm). */
+ASC_SB_API int asc_sb_plan_spmm_stage_rows(asc_sb_context* context, const asc_sb_plan* plan,
+                                           int64_t k, int64_t* rows);
 /* The last asc_sb_plan_spmm_autotune's table: *count candidates in the order
  * timed (R as returned by the autotuner) and their ms per product; up to
  * `capacity` of them are copied. */

@@ -24,7 +24,7 @@ import torch
 import oracle
 from asc_cpp_b200 import synthetic
 from asc_cpp_b200._abi import (PLAN_HAS_BLOCKS16, PLAN_HAS_STAGED_SPMM, PLAN_ROW_GROUPS,
-                               PLAN_TRANSPOSE, SPMM_STAGED, Determinism,
+                               PLAN_TRANSPOSE, Determinism,
                                SparseBlasTranspose, Variant)
 from asc_cpp_b200.sparse_cuda import (CsrPlan, CudaBatch, CudaCsrArray, CudaCsrSpmv,
                                       CudaCsrSpmvWorkspaceSize, CudaSpmm, CudaSpmv,
@@ -183,16 +183,16 @@ def test_stencil_128_spmm(cuda_lib, restatement, k):
     want = oracle.standard_spmm_rows(restatement, a_h.cols, a_h.ptr, a_h.idx, a_h.val, alpha, b,
                                      np.zeros((a_h.rows, k), np.float32))
     assert bits_equal(got, want)
-    # the TMA-staged kernel (16-row groups) at full size, bit for bit too
+    # the TMA-staged kernel at full size (the plan's default for k >= 8), on
+    # the level its stages fit best -- wide groups of 64 rows at k = 8, of 32
+    # at k = 32, the 16-row groups at k = 128 -- bit for bit too
     staged = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
     assert staged.properties() & PLAN_HAS_STAGED_SPMM
-    staged.set_spmm(SPMM_STAGED)
+    assert staged.spmm_stage_rows(k) == {8: 64, 32: 32, 128: 16}[k]
     assert bits_equal(run_spmm(ctx, a, b_d, a_h.rows, a_h.cols, k, alpha, staged), want)
-    staged.close()
     del got, want
     ctx.set_determinism(Determinism.kBackendDefault)
-    for use_plan in (False, True):
-        plan = CsrPlan(ctx, a) if use_plan else None
+    for plan in (None, CsrPlan(ctx, a), staged):
         got = run_spmm(ctx, a, b_d, a_h.rows, a_h.cols, k, alpha, plan)
         spmm_default_check(restatement, a_h, b, got, alpha,
                            lambda n, s: oracle.gamma(n + 2, np.float32) * s)

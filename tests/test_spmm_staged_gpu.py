@@ -186,6 +186,7 @@ def test_stages_beyond_shared_memory_fall_back(cuda_lib, restatement):
     plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
     assert plan.properties() & PLAN_HAS_STAGED_SPMM
     plan.set_spmm(SPMM_STAGED)
+    assert plan.spmm_stage_rows(4) == 0 and plan.spmm_stage_rows(128) == 0
     for k in (4, 128):
         b = rng.standard_normal((cols, k)).astype(np.float32)
         c0 = rng.standard_normal((n, k)).astype(np.float32)
@@ -209,5 +210,50 @@ def test_staged_bounded_wait_status_clean(cuda_lib):
                  DenseMatrixView(c, a_h.rows, 32), plan=plan)
     torch.cuda.synchronize()
     assert ctx.device_status() == 0
+    plan.close()
+    ctx.close()
+
+
+# level (rows per group) the staged kernel runs on for a 27-point 40^3 stencil
+# per k: of the levels whose two stages fit a CTA's shared memory (B200: 227
+# KB), the one with the most CTAs per SM (228 KB per SM), the widest among
+# equals (stage sizes from the groups' slot and entry counts)
+LEVELS_40 = {np.float32: {4: 64, 16: 64, 32: 32, 128: 16},
+             np.float64: {4: 64, 16: 32, 32: 16, 64: 16}}
+
+
+@pytest.mark.parametrize("dt", [np.float32, np.float64], ids=["f32", "f64"])
+def test_stage_levels_bit_exact(cuda_lib, restatement, dt):
+    """The staged kernel runs on wide groups of 64 or 32 rows (the columns
+    their 16-row groups share merged into one slot: fewer, longer copies of
+    B) or on the 16-row groups, by k; every level bit-exact."""
+    rng = np.random.default_rng(21)
+    ctx = context()
+    a_h = synthetic.stencil_27(40, seed=6, dtype=dt)  # 64 000 rows
+    a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+    plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+    plan.set_spmm(SPMM_STAGED)
+    for k, rows in LEVELS_40[dt].items():
+        assert plan.spmm_stage_rows(k) == rows, k
+        b = rng.standard_normal((a_h.cols, k)).astype(dt)
+        c0 = rng.standard_normal((a_h.rows, k)).astype(dt)
+        want = reference(restatement, a_h, b, c0, 0.625)
+        assert bits_equal(run(ctx, plan, a, b, c0, 0.625), want), k
+    assert ctx.device_status() == 0
+    plan.close()
+    ctx.close()
+
+
+def test_stage_rows_zero_where_staging_does_not_apply(cuda_lib):
+    ctx = context()
+    a_h = synthetic.stencil_27(12, seed=7, dtype=np.float32)
+    a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+    plain = CsrPlan(ctx, a, 0)
+    assert plain.spmm_stage_rows(32) == 0  # no staged tables
+    plain.close()
+    plan = CsrPlan(ctx, a, PLAN_ROW_GROUPS)
+    assert plan.spmm_stage_rows(6) == 0    # rows of B not whole 16-byte chunks
+    assert plan.spmm_stage_rows(1024) == 0  # more than 128 chunks per row
+    assert plan.spmm_stage_rows(32) == 32
     plan.close()
     ctx.close()
