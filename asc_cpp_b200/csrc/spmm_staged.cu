@@ -4,19 +4,23 @@
 // and stencil matrices share most of their columns, and the columns of a few
 // consecutive rows form a handful of contiguous runs (a 27-point stencil: 9
 // runs of R + 2 columns for R rows).  A plan (ascb_staged_build) cuts the
-// rows into groups of 16 and records, per group, its distinct columns as
-// "slots" in column order, the maximal runs of consecutive columns among them
-// ("segments"), and per stored entry the slot of its column (16 bits).
+// rows into groups -- 16 rows, and wide groups of 32 and 64 rows that merge
+// the columns two or four 16-row groups share -- and records, per group, its
+// distinct columns as "slots" in column order, the maximal runs of
+// consecutive columns among them ("segments"), and per stored entry the slot
+// of its column (16 bits).
 //
 // The kernel runs a two-stage TMA pipeline per CTA over stages of NG
 // consecutive groups: while it computes stage s, one warp has the bulk copies
 // of stage s+1 in flight -- every segment's rows of B (one cp.async.bulk per
-// segment when ldb == k), the stage's row offsets, values and entry slots --
-// completing on the stage's mbarrier.  Compute reads only shared memory: G
-// lanes own a row's 16-byte chunks of C and walk its entries in stored order,
-// each entry one shared-memory vector load of B(slot, chunk).  So B crosses
-// L2 -> SM once per group and slot instead of once per entry, and no load
-// waits on global memory during compute.
+// segment when ldb == k), the stage's row offsets, values and entry slots,
+// and its rows of C when they are long -- completing on the stage's mbarrier;
+// that warp reads the tables that place the copies two stages ahead.
+// Compute reads only shared memory: G lanes own a row's 16-byte chunks of C
+// and walk its entries in stored order, each entry one shared-memory vector
+// load of B(slot, chunk).  So B crosses L2 -> SM once per group and slot
+// instead of once per entry, and no load waits on global memory during
+// compute (but for short rows of C).
 //
 // Arithmetic per entry, in stored order:
 //   EXACT: C(o,j) = C(o,j) + (alpha*v)*B(c,j), every product and sum rounded

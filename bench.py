@@ -633,7 +633,7 @@ def run_gpu(args, rank, world):
 # ---- further workloads (evidence for the other configurations) -------------
 
 EXTRA = ("spmv_powerlaw_4M_f32", "spmv_t_powerlaw_4M_f64", "spmv_t_powerlaw_4M_f32",
-         "spmm_stencil_k8", "spmm_stencil_k32", "spmm_stencil_k128",
+         "spmm_stencil_k8", "spmm_stencil_k32", "spmm_stencil_k128", "spmm_stencil96_k32",
          "spmm_block_k8", "spmm_block_k32", "spmm_block_k128", "batched_banded_4096",
          "sptrsv_laplacian_1M_f64", "sptrsv_stencil27_2M_f64", "sptrsv_powerlaw_4M_f64",
          "sptrsv_random_2M_f64", "sptrsv_random_2M_f32",
@@ -719,7 +719,12 @@ def run_extra(args):
         extra_cfg.update({"rows": a_h.rows, "nnz": a_h.nnz, "op": "transpose" if transpose else "none"})
     elif w.startswith("spmm"):
         k = int(w.rsplit("_k", 1)[1])
-        a_h = synthetic.stencil_27(128) if "stencil" in w else synthetic.block_sparse()
+        # the 27-point stencil on 128^3 (config 3a) or 96^3 (a small case of the
+        # same kernels for profiling), or the 16 x 16 block matrix (config 3b)
+        if "stencil" in w:
+            a_h = synthetic.stencil_27(96 if "stencil96" in w else 128)
+        else:
+            a_h = synthetic.block_sparse()
         with torch.cuda.stream(stream):
             A = sc.CudaCsrArray(a_h.rows, a_h.cols, torch.from_numpy(a_h.ptr).to(dev),
                                 torch.from_numpy(a_h.idx).to(dev), torch.from_numpy(a_h.val).to(dev))
