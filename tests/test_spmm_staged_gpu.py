@@ -3,7 +3,10 @@ matrices whose groups of 16 rows share columns): DETERMINISTIC products equal
 the oracle bit for bit -- every row still adds its entries in stored order --
 for FP32 and FP64, k from 4 to 260, ragged shapes (a row count that is not a
 multiple of 16, empty rows, a long row), padded leading dimensions of B and C
-(one bulk copy per row of B instead of one per segment) and every stage width;
+(one bulk copy per row of B instead of one per segment) and every stage width
+and level (with these shapes the kernel runs on wide groups of 64 rows at
+k <= 16 (FP32) or 8 (FP64), on wide groups of 32 rows at k = 32 (FP32) or 16
+(FP64), and mostly on 16-row groups above, where the stages fit);
 BACKEND_DEFAULT stays within |c - c_ref| <= gamma_{n+2}(|alpha| sum|a b| +
 |c0|) of the long-double oracle; a plan whose stages do not fit shared memory
 for the call's k falls back to the other kernels with the same results."""
