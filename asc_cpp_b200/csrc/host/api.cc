@@ -82,11 +82,11 @@ constexpr std::size_t kContextScratch = 4096;
 struct Partitions {
   const std::int64_t* warp_tiles = nullptr;    // ascb_row_tiles, warp-tile weights
   std::int64_t n_warp = 0;
-  const std::int64_t* merge_bounds = nullptr;  // ascb_merge_bounds pairs
-  std::int64_t n_merge = 0;
   void* split = nullptr;  // row-split block (ascb_split_bytes(nnz, 256) bytes)
   const std::int64_t* seg_tiles = nullptr;  // the segmented kernel's own row tiles
   std::int64_t n_seg = 0;
+  const std::int64_t* merge_tiles = nullptr;  // the merge partition's row tiles (weight 1)
+  std::int64_t n_merge_tiles = 0;
 };
 
 struct asc_sb_plan {
@@ -239,13 +239,16 @@ std::int64_t SegTiles(std::int64_t rows, std::int64_t nnz) {
 std::size_t SegTileBytes(std::int64_t rows, std::int64_t nnz) {
   return RoundUp(static_cast<std::size_t>(SegTiles(rows, nnz) + 1) * 8, 256);
 }
-// Room for either row-tile partition (the segmented kernel's has fewer tiles
+std::int64_t MergeTiles(std::int64_t rows, std::int64_t nnz) {
+  return ascb_row_tile_count(rows, nnz, ascb_merge_tile_items(), ascb_merge_tile_row_weight());
+}
+std::size_t MergeTileBytes(std::int64_t rows, std::int64_t nnz) {
+  return RoundUp(static_cast<std::size_t>(MergeTiles(rows, nnz) + 1) * 8, 256);
+}
+// Room for any row-tile partition (the segmented kernel's has fewer tiles
 // unless rows average more than about 300 entries).
 std::size_t TileBytes(std::int64_t rows, std::int64_t nnz) {
-  return std::max(WarpTileBytes(rows, nnz), SegTileBytes(rows, nnz));
-}
-std::size_t MergeBoundBytes(std::int64_t rows, std::int64_t nnz) {
-  return RoundUp(static_cast<std::size_t>(ascb_merge_tiles(rows, nnz) + 1) * 16, 256);
+  return std::max({WarpTileBytes(rows, nnz), SegTileBytes(rows, nnz), MergeTileBytes(rows, nnz)});
 }
 
 // ---- workspace layout of asc_sb_csr_spmv ----------------------------------
@@ -260,8 +263,7 @@ std::size_t SplitBlockBytes(std::int64_t nnz) {
 }
 std::size_t CompatWorkspaceBytes(const asc_sb_sparse& m) {
   if (m.rows == 0 || m.columns == 0) return 0;
-  return std::max(TileBytes(m.rows, m.nonzeros) + SplitBlockBytes(m.nonzeros),
-                  MergeBoundBytes(m.rows, m.nonzeros));
+  return TileBytes(m.rows, m.nonzeros) + SplitBlockBytes(m.nonzeros);
 }
 
 // ROW_SPLIT: a row is split when its tail past the tile window exceeds this
@@ -318,33 +320,35 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
                     "CUDA could not launch the vector CSR SpMV kernel");
   }
   const int exact = choice.variant == ASC_SB_VARIANT_ROW_ORDERED ? 1 : 0;
-  if (choice.variant == ASC_SB_VARIANT_MERGE_PATH) {
-    const std::int64_t tiles = ascb_merge_tiles(a.rows, a.nnz);
-    const std::int64_t* bounds = planned != nullptr ? planned->merge_bounds : nullptr;
-    if (bounds == nullptr && scratch != nullptr) {
-      Status s = Launched(ctx, ascb_merge_bounds(ctx->stream, &a, scratch, tiles),
-                          "CUDA could not launch the merge partition kernel");
-      if (!s.ok()) return s;
-      bounds = scratch;
-    }
-    if (bounds != nullptr) {
-      return Launched(ctx,
-                      ascb_spmv_merge(ctx->stream, dtype, form, exact, &a, alpha, beta, &x, &y,
-                                      bounds, tiles, ctx->sm_count, ctx->status),
-                      "CUDA could not launch the merge SpMV kernel");
-    }
-    // no partition buffer at all (zero-workspace calls): warp tiles with
-    // in-kernel bound search
-  }
-  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) run the register-
-  // segmented kernel, which needs 16-byte aligned index and value arrays, on
-  // its own row tiles (up to 128 rows each); otherwise the scalar-load warp
-  // kernel, with the same numerics, on tiles of at most 32 rows.  Either
-  // partition fits the front of the workspace (fewer tiles for the smaller
-  // row weight).
+  // The register-segmented kernel needs 16-byte aligned index and value
+  // arrays; otherwise every variant but VECTOR runs the scalar-load warp
+  // kernel.
   const bool seg_aligned =
       ((reinterpret_cast<std::uintptr_t>(a.idx) | reinterpret_cast<std::uintptr_t>(a.val)) &
        static_cast<std::uintptr_t>(ascb_spmv_seg_alignment() - 1)) == 0;
+  if (choice.variant == ASC_SB_VARIANT_MERGE_PATH && seg_aligned) {
+    // the merge partition -- equal shares of rows plus nonzeros, one item
+    // each -- run by the segmented kernel's tile body (up to 250 rows a tile)
+    const std::int64_t weight = ascb_merge_tile_row_weight();
+    const std::int64_t items = ascb_merge_tile_items();
+    const std::int64_t tiles = ascb_row_tile_count(a.rows, a.nnz, items, weight);
+    const std::int64_t* tiles_ptr = planned != nullptr ? planned->merge_tiles : nullptr;
+    if (tiles_ptr == nullptr && scratch != nullptr) {
+      Status s = Launched(ctx, ascb_row_tiles(ctx->stream, &a, items, weight, scratch, tiles),
+                          "CUDA could not launch the row-tile partition kernel");
+      if (!s.ok()) return s;
+      tiles_ptr = scratch;
+    }
+    return Launched(ctx,
+                    ascb_spmv_seg_w(ctx->stream, dtype, form, 0, &a, alpha, beta, &x, &y,
+                                    tiles_ptr, tiles, weight, ctx->sm_count),
+                    "CUDA could not launch the segmented SpMV kernel");
+  }
+  // ROW_ORDERED (bit-exact) and WARP_TILES (contracted) run the register-
+  // segmented kernel on its own row tiles (up to 125 rows each) when the
+  // arrays are aligned; otherwise the scalar-load warp kernel, with the same
+  // numerics, on tiles of at most 32 rows.  Any partition fits the front of
+  // the workspace.
   const std::int64_t weight =
       seg_aligned ? ascb_seg_tile_row_weight() : ascb_warp_tile_row_weight();
   const std::int64_t items = seg_aligned ? ascb_seg_tile_items() : ascb_warp_tile_items();
@@ -392,16 +396,17 @@ Status RunCsr(asc_sb_context* ctx, const Choice& choice, int form,
 Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* buffer,
                        Partitions* out) {
   out->n_warp = WarpTiles(a.rows, a.nnz);
-  out->n_merge = ascb_merge_tiles(a.rows, a.nnz);
   auto* warp = reinterpret_cast<std::int64_t*>(buffer);
-  auto* merge = reinterpret_cast<std::int64_t*>(buffer + WarpTileBytes(a.rows, a.nnz));
   out->warp_tiles = warp;
-  out->merge_bounds = merge;
-  out->split = buffer + WarpTileBytes(a.rows, a.nnz) + MergeBoundBytes(a.rows, a.nnz);
+  out->split = buffer + WarpTileBytes(a.rows, a.nnz);
   auto* seg = reinterpret_cast<std::int64_t*>(static_cast<unsigned char*>(out->split) +
                                               SplitBlockBytes(a.nnz));
   out->seg_tiles = seg;
   out->n_seg = SegTiles(a.rows, a.nnz);
+  auto* mtiles = reinterpret_cast<std::int64_t*>(reinterpret_cast<unsigned char*>(seg) +
+                                                 SegTileBytes(a.rows, a.nnz));
+  out->merge_tiles = mtiles;
+  out->n_merge_tiles = MergeTiles(a.rows, a.nnz);
   if (a.rows == 0) return Status::Ok();
   Status s = Launched(ctx,
                       ascb_row_tiles(ctx->stream, &a, ascb_warp_tile_items(),
@@ -413,12 +418,14 @@ Status BuildPartitions(asc_sb_context* ctx, const ascb_csr& a, unsigned char* bu
                               seg, out->n_seg),
                "CUDA could not launch the row-tile partition kernel");
   if (!s.ok()) return s;
-  return Launched(ctx, ascb_merge_bounds(ctx->stream, &a, merge, out->n_merge),
-                  "CUDA could not launch the merge partition kernel");
+  return Launched(ctx,
+                  ascb_row_tiles(ctx->stream, &a, ascb_merge_tile_items(),
+                                 ascb_merge_tile_row_weight(), mtiles, out->n_merge_tiles),
+                  "CUDA could not launch the row-tile partition kernel");
 }
 std::size_t PartitionBytes(std::int64_t rows, std::int64_t nnz) {
-  return WarpTileBytes(rows, nnz) + MergeBoundBytes(rows, nnz) + SplitBlockBytes(nnz) +
-         SegTileBytes(rows, nnz);
+  return WarpTileBytes(rows, nnz) + SplitBlockBytes(nnz) + SegTileBytes(rows, nnz) +
+         MergeTileBytes(rows, nnz);
 }
 
 std::size_t EntryBytes(std::int64_t nnz, std::size_t element) {

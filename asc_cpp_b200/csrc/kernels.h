@@ -70,14 +70,6 @@ int64_t ascb_warp_tile_row_weight(void);
 int ascb_spmv_warp(void* stream, int dtype, int form, int exact, const ascb_csr* a,
                    double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
                    const int64_t* tile_row, int64_t ntiles, int sm_count);
-// Merge-based, TMA-fed SpMV.  bounds[2k], bounds[2k+1] = first row of tile
-// k and ptr[that row], k = 0..ntiles (ascb_merge_bounds).  exact = 1 is
-// bit-exact.  status (nullable) receives 1 if a bounded wait gave up.
-int64_t ascb_merge_tiles(int64_t rows, int64_t nnz);
-int ascb_merge_bounds(void* stream, const ascb_csr* a, int64_t* bounds, int64_t ntiles);
-int ascb_spmv_merge(void* stream, int dtype, int form, int exact, const ascb_csr* a,
-                    double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
-                    const int64_t* bounds, int64_t ntiles, int sm_count, int* status);
 // Register-segmented SpMV over the warp row tiles (exact = 1: bit-exact);
 // requires the column-index and value arrays to start on
 // ascb_spmv_seg_alignment()-byte boundaries.
@@ -94,6 +86,11 @@ int64_t ascb_seg_tile_row_weight(void);
 // than ascb_warp_tile_items() when the weight is small, so that every row of
 // a tile but the first starts inside the tile's 256-position window.
 int64_t ascb_seg_tile_items(void);
+// The merge partition for the segmented kernel (MERGE_PATH): weight 1 (one
+// item per row and one per nonzero), at most ascb_merge_tile_items() items a
+// tile; ascb_spmv_seg_w runs it with exact = 0 only.
+int64_t ascb_merge_tile_row_weight(void);
+int64_t ascb_merge_tile_items(void);
 int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
                     double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
                     int64_t ntiles, int64_t weight, int sm_count);

@@ -40,7 +40,6 @@ constexpr int kRowWeight = kItems / 32;  // the warp-tile partition: at most 32 
 #endif
 constexpr int kSegWeight = ASCB_SEG_ROW_WEIGHT;
 constexpr int kMaxRowsPerLane = kRowWeight / kSegWeight;  // rows per lane in a tile
-constexpr int kMaxRows = 32 * kMaxRowsPerLane;
 static_assert(kRowWeight % kSegWeight == 0 && kMaxRowsPerLane >= 1 && kMaxRowsPerLane <= 8,
               "the segmented kernel's row weight divides 8");
 // A window starts on the aligned position at or before its tile's first
@@ -92,7 +91,7 @@ constexpr unsigned long long kChunkMask = (1ull << 40) - 1;
 template <typename T>
 struct SegSmem {
   uint32_t bits[kItems / 32 + 1];  // row-start bitmap of positions 0..256
-  int16_t rowid[kMaxRows + 1];     // k-th nonempty row of the tile -> its offset
+  int16_t rowid[32 * 8 + 1];       // k-th nonempty row of the tile -> its offset (RPL <= 8)
   int64_t bnd[kChunk + 1];         // first row of tiles c0 .. c0 + kChunk
   alignas(16) T prod[kItems];      // exact form: the window's / a long row's products
 };
@@ -921,6 +920,19 @@ int by_form(cudaStream_t s, int form, const ascb_csr* a, double alpha, double be
               : launch<T, EXACT, false, false, RPL>(s, a, al, be, x, y, tiles, n, sm);
 }
 
+// Contracted tiles only (the merge partition's weight-1 tiles: RPL = 8).
+template <int RPL>
+int seg_rows_fast(void* stream, int dtype, int form, const ascb_csr* a, double alpha,
+                  double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
+                  int64_t ntiles, int sm_count) {
+  auto s = static_cast<cudaStream_t>(stream);
+  if (dtype == ASCB_F64) {
+    return by_form<double, false, RPL>(s, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                       sm_count);
+  }
+  return by_form<float, false, RPL>(s, form, a, alpha, beta, x, y, tile_row, ntiles, sm_count);
+}
+
 template <int RPL>
 int seg_rows(void* stream, int dtype, int form, int exact, const ascb_csr* a, double alpha,
              double beta, const ascb_vec* x, const ascb_vec* y, const int64_t* tile_row,
@@ -953,6 +965,10 @@ extern "C" int64_t ascb_seg_tile_row_weight(void) { return ascb::kSegWeight; }
 extern "C" int64_t ascb_seg_tile_items(void) {
   return ascb::tile_items<ascb::kMaxRowsPerLane>();
 }
+// The merge partition: one item per nonzero and one per row (weight 1), tiles
+// of at most 250 items (up to 250 rows, 8 per lane).
+extern "C" int64_t ascb_merge_tile_row_weight(void) { return 1; }
+extern "C" int64_t ascb_merge_tile_items(void) { return ascb::tile_items<8>(); }
 
 extern "C" int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, const ascb_csr* a,
                                double alpha, double beta, const ascb_vec* x, const ascb_vec* y,
@@ -966,6 +982,10 @@ extern "C" int ascb_spmv_seg_w(void* stream, int dtype, int form, int exact, con
   if (weight == ascb::kSegWeight) {
     return ascb::seg_rows<ascb::kMaxRowsPerLane>(stream, dtype, form, exact, a, alpha, beta, x, y,
                                                  tile_row, ntiles, sm_count);
+  }
+  if (weight == 1 && !exact) {  // the merge partition (contracted only)
+    return ascb::seg_rows_fast<8>(stream, dtype, form, a, alpha, beta, x, y, tile_row, ntiles,
+                                  sm_count);
   }
   return static_cast<int>(cudaErrorInvalidValue);
 }

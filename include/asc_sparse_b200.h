@@ -92,7 +92,10 @@ enum {
   ASC_SB_VARIANT_ROW_ORDERED = 0, /* warp row tiles, bit-exact serial order   */
   ASC_SB_VARIANT_VECTOR = 1,      /* 'lanes' threads per row, shuffle sums    */
   ASC_SB_VARIANT_WARP_TILES = 2,  /* warp row tiles, FMA, parallel long rows  */
-  ASC_SB_VARIANT_MERGE_PATH = 3,  /* merge-path balanced tiles + carry fix-up */
+  ASC_SB_VARIANT_MERGE_PATH = 3,  /* merge-path partition (one item per row
+                                     and per nonzero) on the register-
+                                     segmented tile body; unaligned arrays:
+                                     the warp kernel                          */
   ASC_SB_VARIANT_ROW_SPLIT = 4    /* warp row tiles; long rows' tails split
                                      into 256-entry chunks over many warps   */
 };
