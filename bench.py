@@ -591,6 +591,8 @@ def run_gpu(args, rank, world):
     selection = selector_leg() if rank == 0 and world == 1 and not args.no_selector else None
     peak, peak_kind = _peaks()
     traffic = _traffic_record().get(WORKLOAD)
+    if isinstance(traffic, dict):  # per variant: the one the headline ran
+        traffic = traffic.get(best)
     out = None
     if rank == 0:
         cpu = cpu_baseline_sample(a_h, x_h) if world == 1 else None
