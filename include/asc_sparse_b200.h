@@ -567,7 +567,7 @@ ASC_SB_API int asc_sb_context_set_selector(asc_sb_context* context,
 /* Variant recorded in a plan (selector or autotune); AUTO if none. */
 ASC_SB_API int asc_sb_plan_variant(const asc_sb_plan* plan, int32_t* variant,
                                    int32_t* lanes);
-/* Exhaustive autotune, the selector's fallback and judge: times y = A x with
+/* Exhaustive autotune, the selector's fallback and its yardstick: times y = A x with
  * each candidate (one warm-up, `reps` timed runs, CUDA events on the context
  * stream), writes the mean times to ms[count] (nullable) and records the
  * fastest in the plan.  y is overwritten. */
