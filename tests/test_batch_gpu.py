@@ -91,7 +91,7 @@ def test_batch_default_mode_within_bound(cuda_lib, restatement):
             continue
         exact, absval = restatement.extended(0, m.rows, m.cols, m.ptr, m.idx, m.val, x)
         counts = np.diff(m.ptr)
-        ref = -2.0 * exact.astype(np.float64) + 0.25 * y0
+        ref = -2.0 * exact + 0.25 * y0.astype(np.longdouble)
         assert_within_bound(host(t), exact, absval, counts, np.float64, -2.0,
                             np.abs(0.25 * y0), ref)
     batch.close()

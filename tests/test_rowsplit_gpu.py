@@ -51,7 +51,7 @@ def test_row_split_long_rows_within_bound_and_repeatable(cuda_lib, restatement, 
     exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val,
                                          x_h)
     counts = np.diff(a_h.ptr)
-    ref = alpha * exact.astype(np.float64) + beta * y0.astype(np.float64)
+    ref = alpha * exact + beta * y0.astype(np.longdouble)
     ctx = context(Determinism.kBackendDefault)
     a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
     x = dev(x_h)
@@ -89,7 +89,7 @@ def test_row_split_standard_form_through_plan(cuda_lib, restatement):
     exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val,
                                          x_h)
     counts = np.diff(a_h.ptr)
-    ref = y0 + alpha * exact.astype(np.float64)
+    ref = y0.astype(np.longdouble) + alpha * exact
     ctx = context(Determinism.kBackendDefault)
     ctx.set_variant(Variant.kRowSplit, 1)
     a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)

@@ -114,7 +114,7 @@ def test_autotune_picks_the_fastest_and_plan_uses_it(cuda_lib, restatement):
     yt = dev(y0)
     plan.csr_spmv(1.25, vec(x, writable=False), 0.5, vec(yt))
     exact, absval = restatement.extended(0, m.rows, m.cols, m.ptr, m.idx, m.val, x_h)
-    ref = 1.25 * exact.astype(np.float64) + 0.5 * y0
+    ref = 1.25 * exact + 0.5 * y0.astype(np.longdouble)
     assert_within_bound(host(yt), exact, absval, np.diff(m.ptr), np.float64, 1.25,
                         np.abs(0.5 * y0), ref)
     plan.close()
@@ -141,7 +141,7 @@ def test_installed_selector_picks_a_variant(cuda_lib, restatement):
         exact, absval = restatement.extended(0, m64.rows, m64.cols, m64.ptr, m64.idx, m64.val,
                                              x_h)
         assert_within_bound(host(y), exact, absval, np.diff(m64.ptr), np.float64, 1.0,
-                            np.zeros(m64.rows), exact.astype(np.float64))
+                            np.zeros(m64.rows), exact)
         plan.close()
     # DETERMINISTIC contexts ignore the selector: plans record no variant
     ctx.set_determinism(Determinism.kDeterministic)

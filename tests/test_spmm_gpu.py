@@ -89,9 +89,10 @@ def test_transposed_spmm_default_mode_within_bound(cuda_lib, restatement):
         bj = np.ascontiguousarray(b[:, j])
         exact, absval = restatement.extended(OP_TRANSPOSE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
                                              a_h.val, bj)
-        ref = c0[:, j] + exact.astype(np.float64)
+        ref = c0[:, j].astype(np.longdouble) + exact  # long double: exact to the bound
         bound = gamma(counts + 2, np.float64) * (absval.astype(np.float64) + np.abs(c0[:, j]))
-        assert np.all(np.abs(out[:, j] - ref) <= bound + 1e-300)
+        err = np.abs(out[:, j].astype(np.longdouble) - ref).astype(np.float64)
+        assert np.all(err <= bound + 1e-300)
     ctx.close()
 
 
@@ -127,9 +128,9 @@ def test_row_major_default_mode_within_bound(cuda_lib, restatement, dt, k):
         bj = np.ascontiguousarray(b[:, j])
         exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
                                              a_h.val, bj)
-        ref = c0[:, j].astype(np.float64) - 1.5 * exact.astype(np.float64)
+        ref = c0[:, j].astype(np.longdouble) - 1.5 * exact  # long double
         bound = gamma(counts + 2, dt) * (1.5 * absval.astype(np.float64) +
                                          np.abs(c0[:, j].astype(np.float64)))
-        err = np.abs(out[:, j].astype(np.float64) - ref)
+        err = np.abs(out[:, j].astype(np.longdouble) - ref).astype(np.float64)
         assert np.all(err <= bound + np.finfo(dt).tiny), j
     ctx.close()

@@ -193,7 +193,7 @@ def test_vector_variant_within_bound(cuda_lib, restatement, tag, dt, lanes):
     alpha, beta = 1.25, -0.5
     y = dev(y0)
     compat(ctx, a, alpha, dev(x_h), beta, y)
-    ref = alpha * exact.astype(np.float64) + beta * y0.astype(np.float64)
+    ref = alpha * exact + beta * y0.astype(np.longdouble)
     assert_within_bound(host(y), exact, absval, counts, dt, alpha,
                         np.abs(beta * y0.astype(np.float64)), ref)
     ctx.close()
@@ -212,7 +212,7 @@ def test_transpose_default_mode_within_bound(cuda_lib, restatement, tag, dt):
     exact, absval = restatement.extended(OP_TRANSPOSE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
                                          a_h.val, x_h)
     counts = restatement.output_counts(OP_TRANSPOSE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx)
-    ref = y0.astype(np.float64) + 0.75 * exact.astype(np.float64)
+    ref = y0.astype(np.longdouble) + 0.75 * exact
     assert_within_bound(host(y), exact, absval, counts, dt, 0.75,
                         np.abs(y0.astype(np.float64)), ref)
     # CSC with op = none is the same product on the same arrays
@@ -343,8 +343,11 @@ def _shapes(rng, dt):
 
 
 @pytest.mark.parametrize("tag,dt", DTYPES)
-def test_merge_variant_within_bound(cuda_lib, restatement, tag, dt):
-    """MERGE_PATH (contracted) stays inside the error bound on every shape."""
+@pytest.mark.parametrize("misalign", [False, True])
+def test_merge_variant_within_bound(cuda_lib, restatement, tag, dt, misalign):
+    """MERGE_PATH (contracted: the merge partition on the segmented tile
+    body; the scalar-load kernel when the arrays are not 16-byte aligned)
+    stays inside the error bound on every shape."""
     rng = np.random.default_rng(21)
     ctx = context(Determinism.kBackendDefault)
     ctx.set_variant(Variant.kMergePath)
@@ -352,19 +355,25 @@ def test_merge_variant_within_bound(cuda_lib, restatement, tag, dt):
         x_h = rng.uniform(-1, 1, a_h.cols).astype(dt)
         y0 = rng.uniform(-1, 1, a_h.rows).astype(dt)
         a = csr(a_h.rows, a_h.cols, a_h.ptr, a_h.idx, a_h.val)
+        if misalign:  # idx/val views starting 8 (resp. 4) bytes into a buffer
+            idx_store = torch.zeros(a_h.nnz + 1, dtype=torch.int64, device="cuda")
+            val_store = torch.zeros(a_h.nnz + 1, dtype=a.values.dtype, device="cuda")
+            idx_store[1:] = a.indices
+            val_store[1:] = a.values
+            a.indices, a.values = idx_store[1:], val_store[1:]
         exact, absval = restatement.extended(OP_NONE, a_h.rows, a_h.cols, a_h.ptr, a_h.idx,
                                              a_h.val, x_h)
         counts = np.diff(a_h.ptr)
         for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
             y = dev(y0)
             compat(ctx, a, alpha, dev(x_h), beta, y)
-            ref = alpha * exact.astype(np.float64) + beta * y0.astype(np.float64)
+            ref = alpha * exact + beta * y0.astype(np.longdouble)
             assert_within_bound(host(y), exact, absval, counts, dt, alpha,
                                 np.abs(beta * y0.astype(np.float64)), ref)
             y = dev(y0)
             CudaSpmv(ctx, SparseBlasTranspose.kNone, alpha, a, vec(dev(x_h), writable=False),
                      vec(y))
-            ref = y0.astype(np.float64) + alpha * exact.astype(np.float64)
+            ref = y0.astype(np.longdouble) + alpha * exact
             assert_within_bound(host(y), exact, absval, counts, dt, alpha,
                                 np.abs(y0.astype(np.float64)), ref)
     assert ctx.device_status() == 0
@@ -395,13 +404,13 @@ def test_warp_tiles_variant_within_bound(cuda_lib, restatement, tag, dt, misalig
         for alpha, beta in ((1.0, 0.0), (-0.75, 1.5)):
             y = dev(y0)
             compat(ctx, a, alpha, dev(x_h), beta, y)
-            ref = alpha * exact.astype(np.float64) + beta * y0.astype(np.float64)
+            ref = alpha * exact + beta * y0.astype(np.longdouble)
             assert_within_bound(host(y), exact, absval, counts, dt, alpha,
                                 np.abs(beta * y0.astype(np.float64)), ref)
             y = dev(y0)
             CudaSpmv(ctx, SparseBlasTranspose.kNone, alpha, a, vec(dev(x_h), writable=False),
                      vec(y))
-            ref = y0.astype(np.float64) + alpha * exact.astype(np.float64)
+            ref = y0.astype(np.longdouble) + alpha * exact
             assert_within_bound(host(y), exact, absval, counts, dt, alpha,
                                 np.abs(y0.astype(np.float64)), ref)
     ctx.close()
