@@ -561,12 +561,14 @@ def error_report(got, reference, absval, counts, dtype, alpha, beta_abs=0.0,
         |y - y_ref| <= gamma_{n+2}(|alpha| sum|a x| + |beta y0|) + tiny
     (plus ``reference_abs_err``, the reference's own error bound, when the
     reference is not exact).  ``max_ratio_to_bound`` <= 1 means within."""
-    got = np.asarray(got, np.float64)
+    # the difference in long double, so a long-double reference is not
+    # rounded to FP64 before it is compared
+    err = np.abs(np.asarray(got, np.longdouble) -
+                 np.asarray(reference, np.longdouble)).astype(np.float64)
     ref = np.asarray(reference, np.float64)
     bound = gamma(np.asarray(counts) + 2, dtype) * (
         abs(alpha) * np.asarray(absval, np.float64) + beta_abs)
     bound = bound + reference_abs_err + np.finfo(dtype).tiny
-    err = np.abs(got - ref)
     scale = np.maximum(np.abs(ref), np.finfo(np.float64).tiny)
     return {"max_abs": float(err.max()) if err.size else 0.0,
             "max_rel": float((err / scale).max()) if err.size else 0.0,
